@@ -1,0 +1,570 @@
+// Implementation of the C ABI declared in include/gpuheipa.h.
+#include "../../include/gpuheipa.h"
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "../host/generators.h"
+#include "../host/metis_io.h"
+#include "solver.cuh"
+
+struct hp_ctx {
+    hp::Ctx c;
+    hp::SolveStats last;
+};
+
+struct hp_graph {
+    hp::DGraph g;
+    size_t front_mark = 0;  // arena front before this graph was allocated
+};
+
+struct hp_jet {
+    hp_ctx *ctx = nullptr;
+    hp::JetLevel L;
+    hp::DistOracle D;
+    bool has_D = false;
+    size_t back_mark = 0, front_mark = 0;
+};
+
+struct hp_host_graph {
+    hp::HostCSR g;
+};
+
+namespace {
+
+template<typename F>
+int guarded(hp_ctx *ctx, F &&f) {
+    try {
+        f();
+        if (ctx) ctx->c.last_error.clear();
+        return HP_OK;
+    } catch (const hp::HpError &e) {
+        if (ctx) ctx->c.last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        if (ctx) ctx->c.last_error = "host allocation failed";
+        return HP_ERR_OOM;
+    } catch (const std::exception &e) {
+        if (ctx) ctx->c.last_error = e.what();
+        return HP_ERR_ARG;
+    }
+}
+
+template<typename F>
+int guarded_host(F &&f) {
+    try {
+        f();
+        return HP_OK;
+    } catch (const hp::HpError &e) {
+        return e.code;
+    } catch (...) {
+        return HP_ERR_ARG;
+    }
+}
+
+std::vector<hp::u32> vec_u32(const uint32_t *p, uint32_t n) { return std::vector<hp::u32>(p, p + n); }
+std::vector<hp::s32> vec_s32(const int32_t *p, uint32_t n) { return std::vector<hp::s32>(p, p + n); }
+
+void check_hier(const uint32_t *hier, const int32_t *dist, uint32_t levels) {
+    if (!hier || !dist || levels == 0) throw hp::HpError{HP_ERR_ARG, "hierarchy and distance are required"};
+}
+
+} // namespace
+
+extern "C" {
+
+int hp_ctx_create(int device, size_t arena_bytes, hp_ctx **out) {
+    if (!out) return HP_ERR_ARG;
+    *out = nullptr;
+    hp_ctx *ctx = new (std::nothrow) hp_ctx();
+    if (!ctx) return HP_ERR_OOM;
+    int rc = guarded(ctx, [&] { ctx->c.init(device, arena_bytes); });
+    if (rc != HP_OK) {
+        ctx->c.destroy();
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return HP_OK;
+}
+
+int hp_ctx_destroy(hp_ctx *ctx) {
+    if (!ctx) return HP_ERR_ARG;
+    ctx->c.destroy();
+    delete ctx;
+    return HP_OK;
+}
+
+const char *hp_last_error(const hp_ctx *ctx) { return ctx ? ctx->c.last_error.c_str() : "null context"; }
+
+size_t hp_arena_estimate(uint32_t n, uint64_t m, int has_ew, int has_vw) {
+    return hp::arena_estimate(n, m, has_ew != 0, has_vw != 0);
+}
+
+size_t hp_arena_peak(const hp_ctx *ctx) { return ctx ? ctx->c.arena.peak() : 0; }
+
+int hp_graph_upload(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj, const int32_t *ew,
+                    const int32_t *vw, hp_graph **out) {
+    if (!ctx || !out) return HP_ERR_ARG;
+    *out = nullptr;
+    hp_graph *h = new (std::nothrow) hp_graph();
+    if (!h) return HP_ERR_OOM;
+    h->front_mark = ctx->c.arena.front_mark();
+    int rc = guarded(ctx, [&] { h->g = hp::graph_upload(ctx->c, n, m, xadj, adj, ew, vw); });
+    if (rc != HP_OK) {
+        ctx->c.arena.front_release(h->front_mark);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return HP_OK;
+}
+
+int hp_graph_free(hp_ctx *ctx, hp_graph *g) {
+    if (!ctx || !g) return HP_ERR_ARG;
+    ctx->c.arena.front_release(g->front_mark);
+    delete g;
+    return HP_OK;
+}
+
+int hp_graph_info(const hp_graph *g, uint32_t *n, uint64_t *m, int64_t *total_vw) {
+    if (!g) return HP_ERR_ARG;
+    if (n) *n = g->g.n;
+    if (m) *m = g->g.m;
+    if (total_vw) *total_vw = g->g.total_vw;
+    return HP_OK;
+}
+
+int hp_graph_download(hp_ctx *ctx, const hp_graph *g, uint32_t *xadj, uint32_t *adj, int32_t *ew, int32_t *vw) {
+    if (!ctx || !g) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        std::vector<hp::u32> tx, ta;
+        std::vector<hp::s32> te;
+        if (!xadj) {
+            tx.resize((size_t) g->g.n + 1);
+            xadj = tx.data();
+        }
+        if (!adj) {
+            ta.resize(g->g.m);
+            adj = ta.data();
+        }
+        if (!ew) {
+            te.resize(g->g.m);
+            ew = te.data();
+        }
+        hp::graph_download(ctx->c, g->g, xadj, adj, ew, vw);
+    });
+}
+
+int hp_match(hp_ctx *ctx, const hp_graph *g, uint32_t *mapping, uint32_t *n_coarse) {
+    if (!ctx || !g || !mapping) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        hp::ScratchScope ss(ctx->c.arena);
+        hp::u32 *d = ctx->c.balloc<hp::u32>(g->g.n);
+        hp::u32 nc = hp::match_graph(ctx->c, g->g, d);
+        HP_CUDA(cudaMemcpyAsync(mapping, d, sizeof(hp::u32) * g->g.n, cudaMemcpyDeviceToHost, ctx->c.stream));
+        ctx->c.sync();
+        if (n_coarse) *n_coarse = nc;
+    });
+}
+
+int hp_contract(hp_ctx *ctx, const hp_graph *g, const uint32_t *mapping, uint32_t n_coarse, hp_graph **out) {
+    if (!ctx || !g || !mapping || !out) return HP_ERR_ARG;
+    *out = nullptr;
+    for (uint32_t u = 0; u < g->g.n; ++u)
+        if (mapping[u] >= n_coarse) {
+            ctx->c.last_error = "mapping value out of range";
+            return HP_ERR_ARG;
+        }
+    hp_graph *h = new (std::nothrow) hp_graph();
+    if (!h) return HP_ERR_OOM;
+    h->front_mark = ctx->c.arena.front_mark();
+    int rc = guarded(ctx, [&] {
+        hp::u32 *d = ctx->c.falloc<hp::u32>(g->g.n);
+        HP_CUDA(cudaMemcpyAsync(d, mapping, sizeof(hp::u32) * g->g.n, cudaMemcpyHostToDevice, ctx->c.stream));
+        h->g = hp::contract_graph(ctx->c, g->g, d, n_coarse);
+        ctx->c.sync();
+    });
+    if (rc != HP_OK) {
+        ctx->c.arena.front_release(h->front_mark);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return HP_OK;
+}
+
+int hp_jet_refine(hp_ctx *ctx, const hp_graph *g, uint32_t k, int32_t lmax, int ultra, uint32_t level,
+                  uint32_t *part, int64_t *obj, int32_t *maxw, const uint32_t *hier, const int32_t *dist,
+                  uint32_t levels) {
+    if (!ctx || !g || !part || !obj || !maxw || k == 0) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        const size_t fm = ctx->c.arena.front_mark();
+        hp::ScratchScope ss(ctx->c.arena);
+        hp::DistOracle D;
+        if (hier) {
+            check_hier(hier, dist, levels);
+            D = hp::make_dist_oracle(ctx->c, vec_u32(hier, levels), vec_s32(dist, levels));
+            if (D.k != k) throw hp::HpError{HP_ERR_ARG, "k must equal the product of the hierarchy"};
+        }
+        for (uint32_t u = 0; u < g->g.n; ++u)
+            if (part[u] >= k) throw hp::HpError{HP_ERR_ARG, "partition label out of range"};
+        hp::u32 *d = ctx->c.balloc<hp::u32>(g->g.n);
+        HP_CUDA(cudaMemcpyAsync(d, part, sizeof(hp::u32) * g->g.n, cudaMemcpyHostToDevice, ctx->c.stream));
+        hp::s64 o = *obj;
+        hp::s32 mw = *maxw;
+        hp::jet_refine(ctx->c, g->g, d, k, lmax, ultra != 0, level, o, mw, hier ? &D : nullptr);
+        HP_CUDA(cudaMemcpyAsync(part, d, sizeof(hp::u32) * g->g.n, cudaMemcpyDeviceToHost, ctx->c.stream));
+        ctx->c.sync();
+        *obj = o;
+        *maxw = mw;
+        ctx->c.arena.front_release(fm);
+    });
+}
+
+int hp_jet_begin(hp_ctx *ctx, const hp_graph *g, uint32_t k, int32_t lmax, const uint32_t *part,
+                 const uint32_t *hier, const int32_t *dist, uint32_t levels, hp_jet **out) {
+    if (!ctx || !g || !part || !out || k == 0) return HP_ERR_ARG;
+    *out = nullptr;
+    hp_jet *j = new (std::nothrow) hp_jet();
+    if (!j) return HP_ERR_OOM;
+    j->ctx = ctx;
+    j->front_mark = ctx->c.arena.front_mark();
+    j->back_mark = ctx->c.arena.back_mark();
+    int rc = guarded(ctx, [&] {
+        if (hier) {
+            check_hier(hier, dist, levels);
+            j->D = hp::make_dist_oracle(ctx->c, vec_u32(hier, levels), vec_s32(dist, levels));
+            j->has_D = true;
+            if (j->D.k != k) throw hp::HpError{HP_ERR_ARG, "k must equal the product of the hierarchy"};
+        }
+        for (uint32_t u = 0; u < g->g.n; ++u)
+            if (part[u] >= k) throw hp::HpError{HP_ERR_ARG, "partition label out of range"};
+        hp::u32 *d = ctx->c.balloc<hp::u32>(g->g.n);
+        HP_CUDA(cudaMemcpyAsync(d, part, sizeof(hp::u32) * g->g.n, cudaMemcpyHostToDevice, ctx->c.stream));
+        j->L.setup(ctx->c, g->g, k, lmax, j->has_D ? &j->D : nullptr, d);
+        ctx->c.sync();
+    });
+    if (rc != HP_OK) {
+        ctx->c.arena.back_release(j->back_mark);
+        ctx->c.arena.front_release(j->front_mark);
+        delete j;
+        return rc;
+    }
+    *out = j;
+    return HP_OK;
+}
+
+static int jet_moves_out(hp_jet *j, uint32_t *moves, uint32_t *count) {
+    hp::Ctx &c = j->ctx->c;
+    const hp::DevStatus &st = c.read_status();
+    if (st.err) throw hp::HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
+    const hp::u32 nm = st.cnt[hp::ST_MOVES];
+    if (count) *count = nm;
+    if (moves && nm) {
+        HP_CUDA(cudaMemcpyAsync(moves, j->L.moves, sizeof(hp::u32) * nm, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        std::sort(moves, moves + nm);
+    }
+    return HP_OK;
+}
+
+int hp_jet_lp(hp_jet *j, uint32_t ratio_pct, uint32_t *moves, uint32_t *count) {
+    if (!j) return HP_ERR_ARG;
+    return guarded(j->ctx, [&] {
+        j->L.lp(ratio_pct);
+        jet_moves_out(j, moves, count);
+    });
+}
+
+int hp_jet_weak(hp_jet *j, uint32_t *moves, uint32_t *count) {
+    if (!j) return HP_ERR_ARG;
+    return guarded(j->ctx, [&] {
+        j->L.weak();
+        jet_moves_out(j, moves, count);
+    });
+}
+
+int hp_jet_strong(hp_jet *j, uint32_t *moves, uint32_t *count) {
+    if (!j) return HP_ERR_ARG;
+    return guarded(j->ctx, [&] {
+        j->L.strong();
+        jet_moves_out(j, moves, count);
+    });
+}
+
+int hp_jet_perform(hp_jet *j, int64_t *obj, int32_t *maxw) {
+    if (!j) return HP_ERR_ARG;
+    return guarded(j->ctx, [&] {
+        j->L.perform();
+        const hp::DevStatus &st = j->ctx->c.read_status();
+        if (st.err) throw hp::HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
+        const hp::s64 d = st.sum[hp::SUM_DELTA];
+        if (obj) *obj += j->has_D ? d : d / 2;
+        if (maxw) *maxw = st.imax[hp::MAX_BW];
+    });
+}
+
+int hp_jet_state(hp_jet *j, uint32_t *map, int32_t *bw, uint32_t *dest_part, int32_t *gain1, uint32_t *lock,
+                 uint32_t *dest_cache, int32_t *gain_cache) {
+    if (!j) return HP_ERR_ARG;
+    return guarded(j->ctx, [&] {
+        hp::Ctx &c = j->ctx->c;
+        const size_t n = j->L.g.n;
+        auto cp = [&](void *dst, const void *src, size_t bytes) {
+            if (dst) HP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+        };
+        cp(map, j->L.map, 4 * n);
+        cp(bw, j->L.bw, 4 * (size_t) j->L.k);
+        cp(dest_part, j->L.dest_part, 4 * n);
+        cp(gain1, j->L.gain1, 4 * n);
+        cp(lock, j->L.lock, 4 * n);
+        cp(dest_cache, j->L.dest_cache, 4 * n);
+        cp(gain_cache, j->L.gain_cache, 4 * n);
+        c.sync();
+    });
+}
+
+int hp_jet_end(hp_jet *j) {
+    if (!j) return HP_ERR_ARG;
+    j->ctx->c.arena.back_release(j->back_mark);
+    j->ctx->c.arena.front_release(j->front_mark);
+    delete j;
+    return HP_OK;
+}
+
+int hp_edge_cut(hp_ctx *ctx, const hp_graph *g, const uint32_t *part, int64_t *cut) {
+    if (!ctx || !g || !part || !cut) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        hp::ScratchScope ss(ctx->c.arena);
+        hp::u32 *d = ctx->c.balloc<hp::u32>(g->g.n);
+        HP_CUDA(cudaMemcpyAsync(d, part, sizeof(hp::u32) * g->g.n, cudaMemcpyHostToDevice, ctx->c.stream));
+        *cut = hp::edge_cut_dev(ctx->c, g->g, d);
+    });
+}
+
+int hp_comm_cost(hp_ctx *ctx, const hp_graph *g, const uint32_t *part, const uint32_t *hier, const int32_t *dist,
+                 uint32_t levels, int64_t *J) {
+    if (!ctx || !g || !part || !J) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        check_hier(hier, dist, levels);
+        const size_t fm = ctx->c.arena.front_mark();
+        hp::ScratchScope ss(ctx->c.arena);
+        hp::DistOracle D = hp::make_dist_oracle(ctx->c, vec_u32(hier, levels), vec_s32(dist, levels));
+        hp::u32 *d = ctx->c.balloc<hp::u32>(g->g.n);
+        HP_CUDA(cudaMemcpyAsync(d, part, sizeof(hp::u32) * g->g.n, cudaMemcpyHostToDevice, ctx->c.stream));
+        *J = hp::comm_cost_dev(ctx->c, g->g, d, D);
+        ctx->c.arena.front_release(fm);
+    });
+}
+
+int hp_partition_graph(hp_ctx *ctx, const hp_graph *g, uint32_t k, double imbalance, int ultra, uint64_t seed,
+                       uint32_t *part, int64_t *cut) {
+    if (!ctx || !g || !part || k == 0) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        const size_t fm = ctx->c.arena.front_mark();
+        hp::u32 *d = ctx->c.falloc<hp::u32>(g->g.n);
+        ctx->last = hp::SolveStats();
+        hp::s64 c = hp::solve_partition(ctx->c, g->g, k, imbalance, ultra != 0, seed, d, &ctx->last);
+        HP_CUDA(cudaMemcpyAsync(part, d, sizeof(hp::u32) * g->g.n, cudaMemcpyDeviceToHost, ctx->c.stream));
+        ctx->c.sync();
+        ctx->c.arena.front_release(fm);
+        if (cut) *cut = c;
+    });
+}
+
+int hp_partition(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj, const int32_t *ew,
+                 const int32_t *vw, uint32_t k, double imbalance, int ultra, uint64_t seed, uint32_t *part,
+                 int64_t *cut) {
+    if (!ctx || !part || k == 0) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        const size_t fm = ctx->c.arena.front_mark();
+        try {
+            hp::DGraph g = hp::graph_upload(ctx->c, n, m, xadj, adj, ew, vw);
+            hp::u32 *d = ctx->c.falloc<hp::u32>(n);
+            ctx->last = hp::SolveStats();
+            hp::s64 c = hp::solve_partition(ctx->c, g, k, imbalance, ultra != 0, seed, d, &ctx->last);
+            HP_CUDA(cudaMemcpyAsync(part, d, sizeof(hp::u32) * n, cudaMemcpyDeviceToHost, ctx->c.stream));
+            ctx->c.sync();
+            if (cut) *cut = c;
+        } catch (...) {
+            ctx->c.arena.front_release(fm);
+            throw;
+        }
+        ctx->c.arena.front_release(fm);
+    });
+}
+
+int hp_map_graph(hp_ctx *ctx, const hp_graph *g, const uint32_t *hier, const int32_t *dist, uint32_t levels,
+                 double imbalance, int mode, uint64_t seed, uint32_t *part, int64_t *J) {
+    if (!ctx || !g || !part || mode < 0 || mode > 2) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        check_hier(hier, dist, levels);
+        const size_t fm = ctx->c.arena.front_mark();
+        hp::u32 *d = ctx->c.falloc<hp::u32>(g->g.n);
+        ctx->last = hp::SolveStats();
+        hp::s64 j = hp::solve_mapping(ctx->c, g->g, vec_u32(hier, levels), vec_s32(dist, levels), imbalance, mode,
+                                      seed, d, &ctx->last);
+        HP_CUDA(cudaMemcpyAsync(part, d, sizeof(hp::u32) * g->g.n, cudaMemcpyDeviceToHost, ctx->c.stream));
+        ctx->c.sync();
+        ctx->c.arena.front_release(fm);
+        if (J) *J = j;
+    });
+}
+
+int hp_map(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj, const int32_t *ew,
+           const int32_t *vw, const uint32_t *hier, const int32_t *dist, uint32_t levels, double imbalance, int mode,
+           uint64_t seed, uint32_t *part, int64_t *J) {
+    if (!ctx || !part || mode < 0 || mode > 2) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        check_hier(hier, dist, levels);
+        const size_t fm = ctx->c.arena.front_mark();
+        try {
+            hp::DGraph g = hp::graph_upload(ctx->c, n, m, xadj, adj, ew, vw);
+            hp::u32 *d = ctx->c.falloc<hp::u32>(n);
+            ctx->last = hp::SolveStats();
+            hp::s64 j = hp::solve_mapping(ctx->c, g, vec_u32(hier, levels), vec_s32(dist, levels), imbalance, mode,
+                                          seed, d, &ctx->last);
+            HP_CUDA(cudaMemcpyAsync(part, d, sizeof(hp::u32) * n, cudaMemcpyDeviceToHost, ctx->c.stream));
+            ctx->c.sync();
+            if (J) *J = j;
+        } catch (...) {
+            ctx->c.arena.front_release(fm);
+            throw;
+        }
+        ctx->c.arena.front_release(fm);
+    });
+}
+
+int hp_last_solve_stats(const hp_ctx *ctx, double *ms5, int64_t *initial_obj, int32_t *lmax, uint32_t *levels) {
+    if (!ctx) return HP_ERR_ARG;
+    const hp::SolveStats &s = ctx->last;
+    if (ms5) {
+        ms5[0] = s.coarsening_ms;
+        ms5[1] = s.contraction_ms;
+        ms5[2] = s.initial_ms;
+        ms5[3] = s.uncontraction_ms;
+        ms5[4] = s.refinement_ms;
+    }
+    if (initial_obj) *initial_obj = s.initial_obj;
+    if (lmax) *lmax = s.lmax;
+    if (levels) *levels = s.levels;
+    return HP_OK;
+}
+
+int hp_instrument(hp_ctx *ctx, int enable) {
+    if (!ctx) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->c.sync();
+        ctx->c.instr.clear();
+        ctx->c.instr.enabled = enable != 0;
+    });
+}
+
+int hp_kernel_timing(hp_ctx *ctx, const char *name, uint64_t *launches, double *ms, double *bytes) {
+    if (!ctx || !name) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        ctx->c.sync();
+        ctx->c.instr.resolve();
+        uint64_t l = 0;
+        double t = 0, b = 0;
+        for (const auto &x: ctx->c.instr.totals)
+            if (x.name == name) {
+                l = x.launches;
+                t = x.ms;
+                b = x.bytes;
+            }
+        if (launches) *launches = l;
+        if (ms) *ms = t;
+        if (bytes) *bytes = b;
+    });
+}
+
+int hp_read_metis(const char *path, hp_host_graph **out) {
+    if (!path || !out) return HP_ERR_ARG;
+    *out = nullptr;
+    hp_host_graph *h = new (std::nothrow) hp_host_graph();
+    if (!h) return HP_ERR_OOM;
+    std::string err;
+    if (hp::read_metis(path, h->g, err) != 0) {
+        delete h;
+        return HP_ERR_IO;
+    }
+    *out = h;
+    return HP_OK;
+}
+
+int hp_gen_grid(uint32_t w, uint32_t h, int32_t w_lo, int32_t w_hi, uint64_t seed, hp_host_graph **out) {
+    if (!out) return HP_ERR_ARG;
+    return guarded_host([&] { *out = new hp_host_graph{hp::gen_grid(w, h, w_lo, w_hi, seed)}; });
+}
+
+int hp_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, int32_t w_lo, int32_t w_hi,
+                uint64_t seed, int explicit_vw, hp_host_graph **out) {
+    if (!out || scale > 31) return HP_ERR_ARG;
+    return guarded_host([&] {
+        *out = new hp_host_graph{hp::gen_rmat(scale, edge_factor, a, b, c, w_lo, w_hi, seed, explicit_vw != 0)};
+    });
+}
+
+int hp_gen_rgg3d(uint32_t n, double mean_degree, int32_t w_lo, int32_t w_hi, uint64_t seed, int explicit_vw,
+                 hp_host_graph **out) {
+    if (!out || n < 2) return HP_ERR_ARG;
+    return guarded_host(
+        [&] { *out = new hp_host_graph{hp::gen_rgg3d(n, mean_degree, w_lo, w_hi, seed, explicit_vw != 0)}; });
+}
+
+int hp_host_graph_info(const hp_host_graph *g, uint32_t *n, uint64_t *m, int *has_ew, int *has_vw) {
+    if (!g) return HP_ERR_ARG;
+    if (n) *n = g->g.n;
+    if (m) *m = g->g.m;
+    if (has_ew) *has_ew = !g->g.ew.empty();
+    if (has_vw) *has_vw = !g->g.vw.empty();
+    return HP_OK;
+}
+
+int hp_host_graph_copy(const hp_host_graph *g, uint32_t *xadj, uint32_t *adj, int32_t *ew, int32_t *vw) {
+    if (!g) return HP_ERR_ARG;
+    const hp::HostCSR &h = g->g;
+    if (xadj) std::copy(h.xadj.begin(), h.xadj.end(), xadj);
+    if (adj) std::copy(h.adj.begin(), h.adj.end(), adj);
+    if (ew) {
+        if (h.ew.empty()) std::fill(ew, ew + h.m, 1);
+        else std::copy(h.ew.begin(), h.ew.end(), ew);
+    }
+    if (vw) {
+        if (h.vw.empty()) std::fill(vw, vw + h.n, 1);
+        else std::copy(h.vw.begin(), h.vw.end(), vw);
+    }
+    return HP_OK;
+}
+
+int hp_host_graph_free(hp_host_graph *g) {
+    delete g;
+    return HP_OK;
+}
+
+int hp_write_metis(const char *path, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                   const int32_t *ew, const int32_t *vw) {
+    if (!path || !xadj || (m && !adj)) return HP_ERR_ARG;
+    return guarded_host([&] {
+        hp::HostCSR g;
+        g.n = n;
+        g.m = (hp::u32) m;
+        g.xadj.assign(xadj, xadj + n + 1);
+        g.adj.assign(adj, adj + m);
+        if (ew) g.ew.assign(ew, ew + m);
+        if (vw) g.vw.assign(vw, vw + n);
+        std::string err;
+        if (hp::write_metis(path, g, vw != nullptr, ew != nullptr, err) != 0) throw hp::HpError{HP_ERR_IO, err};
+    });
+}
+
+int hp_write_partition(const char *path, const uint32_t *part, uint32_t n) {
+    if (!path || (n && !part)) return HP_ERR_ARG;
+    std::string err;
+    return hp::write_partition(path, part, n, err) == 0 ? HP_OK : HP_ERR_IO;
+}
+
+} // extern "C"

@@ -1,0 +1,156 @@
+#include "context.h"
+
+namespace hp {
+
+static constexpr size_t ALIGN = 256;
+
+static size_t align_up(size_t x) { return (x + ALIGN - 1) & ~(ALIGN - 1); }
+
+void Arena::init(size_t bytes) {
+    bytes = align_up(bytes);
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw HpError{HP_ERR_OOM, "device arena of " + std::to_string(bytes) + " bytes could not be allocated: " +
+                                      cudaGetErrorString(e)};
+    }
+    base_ = (char *) p;
+    size_ = bytes;
+    front_ = 0;
+    back_ = bytes;
+    peak_ = 0;
+}
+
+void Arena::destroy() {
+    if (base_) cudaFree(base_);
+    base_ = nullptr;
+    size_ = front_ = back_ = peak_ = 0;
+}
+
+void *Arena::front(size_t bytes) {
+    bytes = align_up(bytes == 0 ? 1 : bytes);
+    if (front_ + bytes > back_)
+        throw HpError{HP_ERR_OOM, "device arena exhausted (front request " + std::to_string(bytes) + " bytes, " +
+                                      std::to_string(back_ - front_) + " free of " + std::to_string(size_) + ")"};
+    void *p = base_ + front_;
+    front_ += bytes;
+    if (used() > peak_) peak_ = used();
+    return p;
+}
+
+void *Arena::back(size_t bytes) {
+    bytes = align_up(bytes == 0 ? 1 : bytes);
+    if (back_ < front_ + bytes)
+        throw HpError{HP_ERR_OOM, "device arena exhausted (scratch request " + std::to_string(bytes) + " bytes, " +
+                                      std::to_string(back_ - front_) + " free of " + std::to_string(size_) + ")"};
+    back_ -= bytes;
+    if (used() > peak_) peak_ = used();
+    return base_ + back_;
+}
+
+void Ctx::init(int dev, size_t arena_bytes) {
+    device = dev;
+    HP_CUDA(cudaSetDevice(dev));
+    HP_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev));
+    HP_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    HP_CUDA(cudaMalloc(&d_status, sizeof(DevStatus)));
+    HP_CUDA(cudaHostAlloc(&h_status, sizeof(DevStatus), cudaHostAllocDefault));
+    HP_CUDA(cudaMemsetAsync(d_status, 0, sizeof(DevStatus), stream));
+    if (arena_bytes) arena.init(arena_bytes);
+}
+
+cudaEvent_t Instr::get_event() {
+    if (!pool.empty()) {
+        cudaEvent_t e = pool.back();
+        pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    HP_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void Instr::begin(cudaStream_t s, const char *name, double bytes) {
+    if (!enabled) return;
+    Rec r;
+    r.name = name;
+    r.a = get_event();
+    r.b = get_event();
+    r.bytes = bytes;
+    HP_CUDA(cudaEventRecord(r.a, s));
+    pending.push_back(r);
+}
+
+void Instr::end(cudaStream_t s) {
+    if (!enabled || pending.empty()) return;
+    HP_CUDA(cudaEventRecord(pending.back().b, s));
+}
+
+void Instr::resolve() {
+    for (Rec &r: pending) {
+        float ms = 0.f;
+        HP_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        Total *t = nullptr;
+        for (Total &x: totals)
+            if (x.name == r.name) t = &x;
+        if (!t) {
+            totals.push_back(Total{r.name});
+            t = &totals.back();
+        }
+        t->launches += 1;
+        t->ms += ms;
+        t->bytes += r.bytes;
+        pool.push_back(r.a);
+        pool.push_back(r.b);
+    }
+    pending.clear();
+}
+
+void Instr::clear() {
+    for (Rec &r: pending) {
+        pool.push_back(r.a);
+        pool.push_back(r.b);
+    }
+    pending.clear();
+    totals.clear();
+}
+
+void Instr::destroy() {
+    clear();
+    for (cudaEvent_t e: pool) cudaEventDestroy(e);
+    pool.clear();
+}
+
+void Ctx::destroy() {
+    if (stream) cudaStreamSynchronize(stream);
+    instr.destroy();
+    arena.destroy();
+    if (d_status) cudaFree(d_status);
+    if (h_status) cudaFreeHost(h_status);
+    if (stream) cudaStreamDestroy(stream);
+    d_status = nullptr;
+    h_status = nullptr;
+    stream = nullptr;
+}
+
+void Ctx::zero_status() { HP_CUDA(cudaMemsetAsync(d_status, 0, sizeof(DevStatus), stream)); }
+
+void Ctx::zero_counters() {
+    HP_CUDA(cudaMemsetAsync((char *) d_status + sizeof(u32), 0, sizeof(DevStatus) - sizeof(u32), stream));
+}
+
+const DevStatus &Ctx::read_status() {
+    HP_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+    HP_CUDA(cudaStreamSynchronize(stream));
+    return *h_status;
+}
+
+void Ctx::sync() { HP_CUDA(cudaStreamSynchronize(stream)); }
+
+void Ctx::check_device_error() {
+    const DevStatus &s = read_status();
+    if (s.err != 0) throw HpError{HP_ERR_DEVICE, "device reported error bits 0x" + std::to_string(s.err)};
+}
+
+} // namespace hp

@@ -1,0 +1,132 @@
+// Execution context: one device, one stream, one device-memory arena and a
+// small pinned status block through which kernels report counts, sums and
+// error bits to the host (one synchronisation per read).
+//
+// The arena replaces the reference's KokkosMemoryStack
+// (src/datastructures/kokkos_memory_stack.h:36-206): one up-front device
+// allocation, LIFO allocation from the front (long-lived: graph hierarchy,
+// mappings, partitions) and from the back (per-phase scratch), 256-byte
+// alignment, and an error return instead of abort() on exhaustion.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace hp {
+
+struct HpError {
+    int code;
+    std::string msg;
+};
+
+#define HP_CUDA(x)                                                                                   \
+    do {                                                                                             \
+        cudaError_t e_ = (x);                                                                        \
+        if (e_ != cudaSuccess)                                                                       \
+            throw ::hp::HpError{::hp::HP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+#define HP_LAUNCH_CHECK() HP_CUDA(cudaGetLastError())
+
+class Arena {
+public:
+    void init(size_t bytes);
+    void destroy();
+    void *front(size_t bytes);
+    void *back(size_t bytes);
+    size_t front_mark() const { return front_; }
+    size_t back_mark() const { return back_; }
+    void front_release(size_t mark) { front_ = mark; }
+    void back_release(size_t mark) { back_ = mark; }
+    size_t capacity() const { return size_; }
+    size_t used() const { return front_ + (size_ - back_); }
+    size_t peak() const { return peak_; }
+    char *base() const { return base_; }
+
+private:
+    char *base_ = nullptr;
+    size_t size_ = 0, front_ = 0, back_ = 0, peak_ = 0;
+};
+
+// Restores the back (scratch) end of the arena when leaving a scope.
+struct ScratchScope {
+    Arena &a;
+    size_t mark;
+    explicit ScratchScope(Arena &ar) : a(ar), mark(ar.back_mark()) {}
+    ~ScratchScope() { a.back_release(mark); }
+};
+
+// Values kernels report to the host; lives in device memory and is copied to
+// a pinned mirror when the host needs it.
+struct DevStatus {
+    u32 err;          // DevErr bits
+    u32 cnt[15];      // list lengths and other counters
+    long long sum[8]; // 64-bit sums (objective deltas, ...)
+    int imax[8];      // maxima (block weights, ...)
+};
+
+// Optional per-kernel timing with CUDA events on the context's stream. When
+// enabled, instrumented launch sites record an event pair and the
+// algorithmic bytes of the launch; resolve() (after a stream sync) turns the
+// pairs into per-name totals.
+struct Instr {
+    struct Rec {
+        std::string name;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    struct Total {
+        std::string name;
+        u64 launches = 0;
+        double ms = 0.0;
+        double bytes = 0.0;
+    };
+    bool enabled = false;
+    std::vector<Rec> pending;
+    std::vector<Total> totals;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get_event();
+    void begin(cudaStream_t s, const char *name, double bytes);
+    void end(cudaStream_t s);
+    void resolve();  // requires the stream to be idle
+    void clear();
+    void destroy();
+};
+
+struct Ctx {
+    int device = 0;
+    int sm_count = NUM_SMS_HINT;
+    cudaStream_t stream = nullptr;
+    Arena arena;
+    DevStatus *d_status = nullptr;
+    DevStatus *h_status = nullptr;
+    std::string last_error;
+    bool owns_arena = true;
+    Instr instr;
+
+    void init(int dev, size_t arena_bytes);
+    void destroy();
+    template<typename T>
+    T *falloc(size_t n) {
+        return (T *) arena.front(sizeof(T) * (n == 0 ? 1 : n));
+    }
+    template<typename T>
+    T *balloc(size_t n) {
+        return (T *) arena.back(sizeof(T) * (n == 0 ? 1 : n));
+    }
+    void zero_status();                 // async, clears everything including err
+    void zero_counters();               // async, keeps err
+    const DevStatus &read_status();     // syncs the stream
+    void sync();
+    void check_device_error();          // reads status; throws on error bits
+    u32 grid(u64 items, u32 per_block) const {
+        u64 b = (items + per_block - 1) / per_block;
+        if (b == 0) b = 1;
+        u64 cap = (u64) sm_count * 16;
+        return (u32) (b > cap ? cap : b);
+    }
+};
+
+} // namespace hp

@@ -1,0 +1,407 @@
+// Graph contraction (src/datastructures/graph.h:127-390) as one aggregation
+// pass over the member rows of every coarse vertex. Coarse rows are
+// aggregated in registers (row capacity <= 16), a per-warp shared-memory hash
+// table (<= 256), a per-block shared-memory table (<= 4096) or a global hash
+// table (larger), and written straight into the padded coarse CSR at the
+// capacity offsets.
+#include "coarsen.cuh"
+#include "prims.cuh"
+
+namespace hp {
+namespace {
+
+constexpr u32 EMPTY = 0xFFFFFFFFu;
+constexpr u32 C_THREAD_MAX = 16;
+constexpr u32 C_WARP_MAX = 256;
+constexpr u32 C_WARP_BITS = 9;  // 512 slots per warp
+constexpr u32 C_WARP_SLOTS = 1u << C_WARP_BITS;
+constexpr u32 C_BLOCK_MAX = 4096;
+constexpr u32 C_BLOCK_BITS = 13;  // 8192 slots per block
+constexpr u32 C_BLOCK_SLOTS = 1u << C_BLOCK_BITS;
+constexpr int C_WARP_BLOCK = 128;  // 4 warps per block for the warp kernel
+constexpr int C_HUGE_BLOCK = 1024;
+
+__device__ __forceinline__ u32 hslot(u32 key, u32 bits) { return (key * 2654435761u) >> (32 - bits); }
+
+__global__ void k_cluster_stats(DGraph g, const u32 *map, u32 *cnt, u32 *capsum, s32 *cw) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x) {
+        const u32 c = map[u];
+        atomicAdd(&cnt[c], 1u);
+        atomicAdd(&capsum[c], g.rowlen[u]);
+        atomicAdd(&cw[c], g_vw(g, u));
+    }
+}
+
+__global__ void k_fill_members(const u32 *map, u32 n, u32 *cursor, u32 *mlist) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+        const u32 pos = atomicAdd(&cursor[map[u]], 1u);
+        mlist[pos] = u;
+    }
+}
+
+struct CArgs {
+    DGraph g;         // fine graph
+    const u32 *map;   // fine -> coarse
+    const u32 *moff;  // member offsets (n_c + 1)
+    const u32 *mlist; // members
+    DGraph c;         // coarse graph (rowptr, rowlen, adj, ew written here)
+    u32 *err;
+    unsigned long long *m_out;
+};
+
+// Thread-per-coarse-vertex aggregation in registers for capacities <= 16;
+// larger coarse vertices are appended to the warp / block / huge lists.
+__global__ void k_contract_small(CArgs a, u32 *wl, u32 *wcnt, u32 *bl, u32 *bcnt, u32 *hl, u32 *hcnt, u32 *hoff,
+                                 unsigned long long *hbump) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    unsigned long long msum = 0;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.c.n; base += stride) {
+        const u32 c = (u32) (base + threadIdx.x);
+        u32 cls = 0;  // 0 none, 1 warp, 2 block, 3 huge
+        u32 cap = 0;
+        if (c < a.c.n) {
+            cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
+            if (cap <= C_THREAD_MAX) {
+                u32 keys[C_THREAD_MAX];
+                s32 ws[C_THREAD_MAX];
+#pragma unroll
+                for (int s = 0; s < (int) C_THREAD_MAX; ++s) {
+                    keys[s] = EMPTY;
+                    ws[s] = 0;
+                }
+                for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
+                    const u32 u = a.mlist[mi];
+                    const u64 beg = a.g.rowptr[u];
+                    const u32 len = a.g.rowlen[u];
+                    for (u32 t = 0; t < len; ++t) {
+                        const u32 cv = a.map[a.g.adj[beg + t]];
+                        if (cv == c) continue;
+                        const s32 w = g_ew(a.g, beg + t);
+                        bool done = false;
+#pragma unroll
+                        for (int s = 0; s < (int) C_THREAD_MAX; ++s)
+                            if (!done && keys[s] == cv) {
+                                ws[s] = wadd(ws[s], w);
+                                done = true;
+                            }
+#pragma unroll
+                        for (int s = 0; s < (int) C_THREAD_MAX; ++s)
+                            if (!done && keys[s] == EMPTY) {
+                                keys[s] = cv;
+                                ws[s] = w;
+                                done = true;
+                            }
+                    }
+                }
+                u64 pos = a.c.rowptr[c];
+                u32 cntu = 0;
+#pragma unroll
+                for (int s = 0; s < (int) C_THREAD_MAX; ++s)
+                    if (keys[s] != EMPTY) {
+                        a.c.adj[pos + cntu] = keys[s];
+                        a.c.ew[pos + cntu] = ws[s];
+                        ++cntu;
+                    }
+                a.c.rowlen[c] = cntu;
+                msum += cntu;
+            } else if (cap <= C_WARP_MAX) {
+                cls = 1;
+            } else if (cap <= C_BLOCK_MAX) {
+                cls = 2;
+            } else {
+                cls = 3;
+            }
+        }
+        u32 s1 = warp_append(wcnt, cls == 1);
+        if (cls == 1) wl[s1] = c;
+        u32 s2 = warp_append(bcnt, cls == 2);
+        if (cls == 2) bl[s2] = c;
+        u32 s3 = warp_append(hcnt, cls == 3);
+        if (cls == 3) {
+            hl[s3] = c;
+            hoff[s3] = (u32) atomicAdd(hbump, (unsigned long long) (2 * cap));
+        }
+    }
+    msum = warp_sum<unsigned long long>(msum);
+    if (lane_id() == 0 && msum) atomicAdd(a.m_out, msum);
+}
+
+// Inserts (cv, w) into an open-addressing table with linear probing.
+__device__ __forceinline__ bool table_insert(u32 *tk, s32 *tw, u32 mask, u32 h, u32 cv, s32 w) {
+    for (u32 probe = 0; probe <= mask; ++probe) {
+        const u32 prev = atomicCAS(&tk[h], EMPTY, cv);
+        if (prev == EMPTY || prev == cv) {
+            atomicAdd(&tw[h], w);
+            return true;
+        }
+        h = (h + 1) & mask;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(C_WARP_BLOCK) k_contract_warp(CArgs a, const u32 *wl, const u32 *wcnt) {
+    __shared__ u32 tk_all[C_WARP_BLOCK / 32][C_WARP_SLOTS];
+    __shared__ s32 tw_all[C_WARP_BLOCK / 32][C_WARP_SLOTS];
+    u32 *tk = tk_all[warp_in_block()];
+    s32 *tw = tw_all[warp_in_block()];
+    const int lane = lane_id();
+    for (u32 s = lane; s < C_WARP_SLOTS; s += 32) {
+        tk[s] = EMPTY;
+        tw[s] = 0;
+    }
+    __syncwarp();
+    const u32 total = *wcnt;
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long msum = 0;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const u32 c = wl[i];
+        for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
+            const u32 u = a.mlist[mi];
+            const u64 beg = a.g.rowptr[u];
+            const u32 len = a.g.rowlen[u];
+            for (u32 t = lane; t < len; t += 32) {
+                const u32 cv = a.map[a.g.adj[beg + t]];
+                if (cv == c) continue;
+                if (!table_insert(tk, tw, C_WARP_SLOTS - 1, hslot(cv, C_WARP_BITS), cv, g_ew(a.g, beg + t)))
+                    set_error(a.err, DEV_ERR_HASH_FULL);
+            }
+        }
+        __syncwarp();
+        const u64 out = a.c.rowptr[c];
+        u32 cntu = 0;
+        for (u32 s0 = 0; s0 < C_WARP_SLOTS; s0 += 32) {
+            const u32 s = s0 + lane;
+            const u32 key = tk[s];
+            const bool has = key != EMPTY;
+            const unsigned mask = __ballot_sync(FULL, has);
+            if (has) {
+                const u32 p = cntu + __popc(mask & ((1u << lane) - 1u));
+                a.c.adj[out + p] = key;
+                a.c.ew[out + p] = tw[s];
+                tk[s] = EMPTY;
+                tw[s] = 0;
+            }
+            cntu += __popc(mask);
+        }
+        if (lane == 0) a.c.rowlen[c] = cntu;
+        msum += cntu;
+        __syncwarp();
+    }
+    if (lane == 0 && msum) atomicAdd(a.m_out, msum);
+}
+
+// Emits the non-empty slots of a block-wide table into the coarse row.
+template<int NT>
+__device__ __forceinline__ u32 block_emit(u32 *tk, s32 *tw, u32 slots, u64 out, u32 *adj, s32 *ew, bool reset,
+                                          u32 *smem_scan) {
+    const u32 per = slots / NT;
+    const u32 s0 = threadIdx.x * per;
+    u32 cnt = 0;
+    for (u32 s = s0; s < s0 + per; ++s) cnt += tk[s] != EMPTY;
+    u32 tot;
+    u32 p = block_exclusive_scan<u32>(cnt, tot, smem_scan);
+    for (u32 s = s0; s < s0 + per; ++s) {
+        const u32 key = tk[s];
+        if (key != EMPTY) {
+            adj[out + p] = key;
+            ew[out + p] = tw[s];
+            ++p;
+            if (reset) {
+                tk[s] = EMPTY;
+                tw[s] = 0;
+            }
+        }
+    }
+    return tot;
+}
+
+__global__ void __launch_bounds__(BLOCK) k_contract_block(CArgs a, const u32 *bl, const u32 *bcnt) {
+    extern __shared__ u32 dsm[];
+    u32 *tk = dsm;
+    s32 *tw = (s32 *) (dsm + C_BLOCK_SLOTS);
+    __shared__ u32 scan_sm[32];
+    for (u32 s = threadIdx.x; s < C_BLOCK_SLOTS; s += blockDim.x) {
+        tk[s] = EMPTY;
+        tw[s] = 0;
+    }
+    __syncthreads();
+    const u32 total = *bcnt;
+    unsigned long long msum = 0;
+    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
+        const u32 c = bl[i];
+        for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
+            const u32 u = a.mlist[mi];
+            const u64 beg = a.g.rowptr[u];
+            const u32 len = a.g.rowlen[u];
+            for (u32 t = threadIdx.x; t < len; t += blockDim.x) {
+                const u32 cv = a.map[a.g.adj[beg + t]];
+                if (cv == c) continue;
+                if (!table_insert(tk, tw, C_BLOCK_SLOTS - 1, hslot(cv, C_BLOCK_BITS), cv, g_ew(a.g, beg + t)))
+                    set_error(a.err, DEV_ERR_HASH_FULL);
+            }
+        }
+        __syncthreads();
+        const u32 cntu = block_emit<BLOCK>(tk, tw, C_BLOCK_SLOTS, a.c.rowptr[c], a.c.adj, a.c.ew, true, scan_sm);
+        if (threadIdx.x == 0) a.c.rowlen[c] = cntu;
+        msum += cntu;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && msum) atomicAdd(a.m_out, msum);
+}
+
+__device__ __forceinline__ u32 range_hash(u32 key, u32 size) {
+    return (u32) (((u64) (key * 2654435761u) * (u64) size) >> 32);
+}
+
+__global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u32 *hl, const u32 *hcnt,
+                                                               const u32 *hoff, u32 *tkeys, s32 *twts) {
+    __shared__ u32 scan_sm[32];
+    const u32 total = *hcnt;
+    unsigned long long msum = 0;
+    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
+        const u32 c = hl[i];
+        const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
+        const u32 tsz = 2 * cap;
+        u32 *tk = tkeys + hoff[i];
+        s32 *tw = twts + hoff[i];
+        for (u32 s = threadIdx.x; s < tsz; s += blockDim.x) {
+            tk[s] = EMPTY;
+            tw[s] = 0;
+        }
+        __syncthreads();
+        for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
+            const u32 u = a.mlist[mi];
+            const u64 beg = a.g.rowptr[u];
+            const u32 len = a.g.rowlen[u];
+            for (u32 t = threadIdx.x; t < len; t += blockDim.x) {
+                const u32 cv = a.map[a.g.adj[beg + t]];
+                if (cv == c) continue;
+                const s32 w = g_ew(a.g, beg + t);
+                u32 h = range_hash(cv, tsz);
+                bool ok = false;
+                for (u32 probe = 0; probe < tsz; ++probe) {
+                    const u32 prev = atomicCAS(&tk[h], EMPTY, cv);
+                    if (prev == EMPTY || prev == cv) {
+                        atomicAdd(&tw[h], w);
+                        ok = true;
+                        break;
+                    }
+                    h = (h + 1 == tsz) ? 0 : h + 1;
+                }
+                if (!ok) set_error(a.err, DEV_ERR_HASH_FULL);
+            }
+        }
+        __syncthreads();
+        // emit in chunks of blockDim.x slots
+        const u64 out = a.c.rowptr[c];
+        u32 cntu = 0;
+        for (u32 s0 = 0; s0 < tsz; s0 += blockDim.x) {
+            const u32 s = s0 + threadIdx.x;
+            const bool has = s < tsz && tk[s] != EMPTY;
+            u32 tot;
+            const u32 p = block_exclusive_scan<u32>(has ? 1u : 0u, tot, scan_sm);
+            if (has) {
+                a.c.adj[out + cntu + p] = tk[s];
+                a.c.ew[out + cntu + p] = tw[s];
+            }
+            cntu += tot;
+        }
+        if (threadIdx.x == 0) a.c.rowlen[c] = cntu;
+        msum += cntu;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && msum) atomicAdd(a.m_out, msum);
+}
+
+} // namespace
+
+DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
+    DGraph c;
+    c.n = n_c;
+    c.cap = g.m;
+    c.total_vw = g.total_vw;
+    c.rowptr = ctx.falloc<u32>((u64) n_c + 1);
+    c.rowlen = ctx.falloc<u32>(n_c);
+    c.vw = ctx.falloc<s32>(n_c);
+    c.adj = ctx.falloc<u32>(c.cap);
+    c.ew = ctx.falloc<s32>(c.cap);
+
+    ScratchScope ss(ctx.arena);
+    u32 *cnt = ctx.balloc<u32>(n_c);
+    u32 *capsum = ctx.balloc<u32>(n_c);
+    u32 *moff = ctx.balloc<u32>((u64) n_c + 1);
+    u32 *cursor = ctx.balloc<u32>(n_c);
+    u32 *mlist = ctx.balloc<u32>(g.n);
+    u32 *wl = ctx.balloc<u32>(n_c);
+    u32 *bl = ctx.balloc<u32>(n_c);
+    u32 *hl = ctx.balloc<u32>(n_c);
+    u32 *hoff = ctx.balloc<u32>(n_c);
+    HP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(u32) * n_c, ctx.stream));
+    HP_CUDA(cudaMemsetAsync(capsum, 0, sizeof(u32) * n_c, ctx.stream));
+    HP_CUDA(cudaMemsetAsync(c.vw, 0, sizeof(s32) * n_c, ctx.stream));
+    k_cluster_stats<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, mapping, cnt, capsum, c.vw);
+    HP_LAUNCH_CHECK();
+    u32 *rowptr = c.rowptr;
+    device_scan<u32>(
+        ctx, (u64) n_c + 1, [=] __device__(u64 i) -> u32 { return i < n_c ? cnt[i] : 0u; },
+        [=] __device__(u64 i, u32 p, u32) {
+            moff[i] = p;
+            if (i < n_c) cursor[i] = p;
+        },
+        (u32 *) nullptr);
+    device_scan<u32>(
+        ctx, (u64) n_c + 1, [=] __device__(u64 i) -> u32 { return i < n_c ? capsum[i] : 0u; },
+        [=] __device__(u64 i, u32 p, u32) { rowptr[i] = p; }, (u32 *) nullptr);
+    k_fill_members<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(mapping, g.n, cursor, mlist);
+    HP_LAUNCH_CHECK();
+
+    ctx.zero_counters();
+    DevStatus *st = ctx.d_status;
+    CArgs a{g, mapping, moff, mlist, c, &st->err, (unsigned long long *) &st->sum[1]};
+    const size_t rec0 = ctx.instr.pending.size();
+    ctx.instr.begin(ctx.stream, "contract", 0.0);
+    k_contract_small<<<ctx.grid(n_c, BLOCK), BLOCK, 0, ctx.stream>>>(
+        a, wl, &st->cnt[0], bl, &st->cnt[1], hl, &st->cnt[2], hoff, (unsigned long long *) &st->sum[0]);
+    HP_LAUNCH_CHECK();
+    ctx.instr.end(ctx.stream);
+    const DevStatus &s1 = ctx.read_status();
+    const u32 nw = s1.cnt[0], nb = s1.cnt[1], nh = s1.cnt[2];
+    const u64 hslots = (u64) s1.sum[0];
+    if (nw) {
+        ctx.instr.begin(ctx.stream, "contract", 0.0);
+        k_contract_warp<<<ctx.grid((u64) nw * 32, C_WARP_BLOCK), C_WARP_BLOCK, 0, ctx.stream>>>(a, wl, &st->cnt[0]);
+        HP_LAUNCH_CHECK();
+        ctx.instr.end(ctx.stream);
+    }
+    if (nb) {
+        const size_t smem = (size_t) C_BLOCK_SLOTS * 8;
+        HP_CUDA(cudaFuncSetAttribute(k_contract_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        ctx.instr.begin(ctx.stream, "contract", 0.0);
+        k_contract_block<<<(u32) std::min<u64>(nb, (u64) ctx.sm_count * 3), BLOCK, smem, ctx.stream>>>(a, bl,
+                                                                                                     &st->cnt[1]);
+        HP_LAUNCH_CHECK();
+        ctx.instr.end(ctx.stream);
+    }
+    if (nh) {
+        u32 *tkeys = ctx.balloc<u32>(hslots);
+        s32 *twts = ctx.balloc<s32>(hslots);
+        ctx.instr.begin(ctx.stream, "contract", 0.0);
+        k_contract_huge<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
+            a, hl, &st->cnt[2], hoff, tkeys, twts);
+        HP_LAUNCH_CHECK();
+        ctx.instr.end(ctx.stream);
+    }
+    const DevStatus &s2 = ctx.read_status();
+    if (s2.err & DEV_ERR_HASH_FULL) throw HpError{HP_ERR_DEVICE, "contraction hash table overflow"};
+    c.m = (u64) s2.sum[1];
+    // algorithmic bytes of the aggregation pass (roofline accounting): member
+    // lists, fine offsets/lengths/weights, fine rows and weights, map gather,
+    // coarse rows, weights and lengths
+    if (ctx.instr.enabled && ctx.instr.pending.size() > rec0) {
+        const double fine_e = g.ew ? 12.0 : 8.0;
+        ctx.instr.pending[rec0].bytes = 12.0 * g.n + fine_e * (double) g.m + 8.0 * n_c + 8.0 * (double) c.m;
+    }
+    return c;
+}
+
+} // namespace hp

@@ -1,0 +1,1296 @@
+// Jet refinement kernels. Semantics: src/refinement/jet_label_propagation.h
+// and src/refinement/promap_jet_label_propagation.h with the deterministic
+// tie rules documented in jet.cuh (lowest block id on best-block ties,
+// mini-bucket order by vertex id, fallback slots in ascending vertex id).
+#include "jet.cuh"
+#include "prims.cuh"
+
+#include <algorithm>
+
+namespace hp {
+namespace {
+
+constexpr u32 JT = 16;             // thread-level rows up to this degree
+constexpr u32 JW = 512;            // warp-level rows up to this degree
+constexpr u32 JW_SLOTS = 1024;     // per-warp table capacity
+constexpr int JW_BLOCK = 128;      // 4 warps per block
+constexpr u32 JB_SLOTS = 16384;    // per-block table capacity (128 KB)
+constexpr int JB_BLOCK = 512;
+constexpr u32 AB_T = 32;           // afterburner / delta thread-level degree
+constexpr u32 EMPTY = NO_BLOCK_ID;
+constexpr u32 NOKEY = 0xFFFFFFFFu;
+
+struct JArgs {
+    DGraph g;
+    u32 k;
+    s32 lmax;
+    s32 g_weight;
+    const u32 *code;     // non-null: process-mapping objective
+    const s32 *bitdist;
+    u32 *map;
+    s32 *bw;
+    u32 *dest_cache;
+    s32 *gain_cache;
+    u32 *lock;
+    u32 *dest_part;
+    s32 *gain1;
+    u32 *moving;
+    u32 epoch;
+    u32 *cand;
+    u32 *moves;
+    u32 *heavy;
+    u32 *heavy2;
+    DevStatus *st;
+};
+
+__device__ __forceinline__ s32 D(const JArgs &a, u32 x, u32 y) { return dist_of(a.code, a.bitdist, x, y); }
+
+// ---- group abstraction: warp (BLK=false) or block (BLK=true) ---------------------
+template<bool BLK>
+struct Grp {
+    static __device__ __forceinline__ u32 tid() { return BLK ? threadIdx.x : (u32) lane_id(); }
+    static __device__ __forceinline__ u32 size() { return BLK ? blockDim.x : 32u; }
+    static __device__ __forceinline__ void sync() {
+        if (BLK) __syncthreads();
+        else __syncwarp();
+    }
+    static __device__ __forceinline__ unsigned long long max_u64(unsigned long long v, unsigned long long *sm) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long y = __shfl_xor_sync(FULL, v, o);
+            v = y > v ? y : v;
+        }
+        if (!BLK) return v;
+        if (lane_id() == 0) sm[warp_in_block()] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long r = 0;
+            for (u32 w = 0; w < (blockDim.x >> 5); ++w) r = sm[w] > r ? sm[w] : r;
+            sm[32] = r;
+        }
+        __syncthreads();
+        v = sm[32];
+        __syncthreads();
+        return v;
+    }
+    static __device__ __forceinline__ long long sum_s64(long long v, long long *sm) {
+        v = warp_sum<long long>(v);
+        if (!BLK) return v;
+        if (lane_id() == 0) sm[warp_in_block()] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long r = 0;
+            for (u32 w = 0; w < (blockDim.x >> 5); ++w) r += sm[w];
+            sm[32] = r;
+        }
+        __syncthreads();
+        v = sm[32];
+        __syncthreads();
+        return v;
+    }
+};
+
+__device__ __forceinline__ u32 thash(u32 key, u32 mask) { return (key * 2654435761u >> 7) & mask; }
+
+__device__ __forceinline__ u32 table_mask_for(u32 len, u32 k, u32 cap) {
+    u32 want = 2 * (len < k ? len : k);
+    u32 t = 64;
+    while (t < want && t < cap) t <<= 1;
+    return t - 1;
+}
+
+// Aggregates conn(u, .) into the group's table (cleared on entry).
+template<bool BLK>
+__device__ __forceinline__ void table_build(const JArgs &a, u32 u, u32 *tk, s32 *tv, u32 mask) {
+    const u64 beg = a.g.rowptr[u];
+    const u32 len = a.g.rowlen[u];
+    for (u32 t = Grp<BLK>::tid(); t < len; t += Grp<BLK>::size()) {
+        const u32 b = a.map[a.g.adj[beg + t]];
+        const s32 w = g_ew(a.g, beg + t);
+        u32 h = thash(b, mask);
+        bool ok = false;
+        for (u32 p = 0; p <= mask; ++p) {
+            const u32 prev = atomicCAS(&tk[h], EMPTY, b);
+            if (prev == EMPTY || prev == b) {
+                atomicAdd(&tv[h], w);
+                ok = true;
+                break;
+            }
+            h = (h + 1) & mask;
+        }
+        if (!ok) set_error(&a.st->err, DEV_ERR_HASH_FULL);
+    }
+    Grp<BLK>::sync();
+}
+
+template<bool BLK>
+__device__ __forceinline__ void table_clear(u32 *tk, s32 *tv, u32 mask) {
+    Grp<BLK>::sync();
+    for (u32 s = Grp<BLK>::tid(); s <= mask; s += Grp<BLK>::size()) {
+        tk[s] = EMPTY;
+        tv[s] = 0;
+    }
+    Grp<BLK>::sync();
+}
+
+// Thread-level connectivity row in registers (degree <= JT).
+struct TRow {
+    u32 b[JT];
+    s32 c[JT];
+};
+
+__device__ __forceinline__ void trow_build(const JArgs &a, u32 u, TRow &r) {
+#pragma unroll
+    for (int s = 0; s < (int) JT; ++s) {
+        r.b[s] = EMPTY;
+        r.c[s] = 0;
+    }
+    const u64 beg = a.g.rowptr[u];
+    const u32 len = a.g.rowlen[u];
+    for (u32 t = 0; t < len; ++t) {
+        const u32 b = a.map[a.g.adj[beg + t]];
+        const s32 w = g_ew(a.g, beg + t);
+        bool done = false;
+#pragma unroll
+        for (int s = 0; s < (int) JT; ++s)
+            if (!done && r.b[s] == b) {
+                r.c[s] = wadd(r.c[s], w);
+                done = true;
+            }
+#pragma unroll
+        for (int s = 0; s < (int) JT; ++s)
+            if (!done && r.b[s] == EMPTY) {
+                r.b[s] = b;
+                r.c[s] = w;
+                done = true;
+            }
+    }
+}
+
+__device__ __forceinline__ unsigned long long cut_key(s32 c, u32 b) {
+    return ((unsigned long long) (u32) c << 32) | (u32) ~b;
+}
+__device__ __forceinline__ unsigned long long delta_key(s32 d, u32 b) {
+    return ((unsigned long long) ((u32) d ^ 0x80000000u) << 32) | (u32) ~b;
+}
+
+// ---- Jet LP best block (jet_lp :193-238 / ProMap_jet_lp :219-263) ------------------
+
+__device__ __forceinline__ void lp_store(const JArgs &a, u32 u, u32 best, s32 gain) {
+    a.gain_cache[u] = gain;
+    a.dest_cache[u] = best;
+    a.dest_part[u] = best;
+}
+
+__device__ __forceinline__ void lp_finish_cut(const JArgs &a, u32 u, s32 own, unsigned long long bk, u32 ratio) {
+    u32 best = NO_MOVE;
+    s32 gain = 0;
+    if (bk) {
+        const s32 bc = (s32) (u32) (bk >> 32);
+        if (bc >= own || (s64) own - (s64) bc < ((s64) ratio * (s64) own) / 100) {
+            best = ~(u32) bk;
+            gain = wsub(bc, own);
+        }
+    }
+    lp_store(a, u, best, gain);
+}
+
+__device__ __forceinline__ void lp_finish_map(const JArgs &a, u32 u, unsigned long long bk) {
+    u32 best = NO_MOVE;
+    s32 gain = 0;
+    if (bk) {
+        const s32 d = (s32) ((u32) (bk >> 32) ^ 0x80000000u);
+        if (d >= 0) {
+            best = ~(u32) bk;
+            gain = d;
+        }
+    }
+    lp_store(a, u, best, gain);
+}
+
+__device__ __forceinline__ void lp_thread(const JArgs &a, u32 u, u32 ratio) {
+    TRow r;
+    trow_build(a, u, r);
+    const u32 o = a.map[u];
+    unsigned long long bk = 0;
+    if (!a.code) {
+        s32 own = 0;
+#pragma unroll
+        for (int s = 0; s < (int) JT; ++s) {
+            if (r.b[s] == EMPTY) continue;
+            if (r.b[s] == o) own = r.c[s];
+            else {
+                unsigned long long k = cut_key(r.c[s], r.b[s]);
+                bk = k > bk ? k : bk;
+            }
+        }
+        lp_finish_cut(a, u, own, bk, ratio);
+    } else {
+#pragma unroll
+        for (int s = 0; s < (int) JT; ++s) {
+            if (r.b[s] == EMPTY || r.b[s] == o) continue;
+            s32 d = 0;
+#pragma unroll
+            for (int t = 0; t < (int) JT; ++t)
+                if (r.b[t] != EMPTY) d = wadd(d, wmul(r.c[t], wsub(D(a, o, r.b[t]), D(a, r.b[s], r.b[t]))));
+            unsigned long long k = delta_key(d, r.b[s]);
+            bk = k > bk ? k : bk;
+        }
+        lp_finish_map(a, u, bk);
+    }
+}
+
+template<bool BLK>
+__device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, u32 *tk, s32 *tv, u32 mask,
+                                         unsigned long long *smu, long long *sms) {
+    table_build<BLK>(a, u, tk, tv, mask);
+    const u32 o = a.map[u];
+    unsigned long long bk = 0;
+    long long own = 0;
+    for (u32 s = Grp<BLK>::tid(); s <= mask; s += Grp<BLK>::size()) {
+        const u32 b = tk[s];
+        if (b == EMPTY) continue;
+        if (b == o) {
+            own = tv[s];
+            continue;
+        }
+        unsigned long long k;
+        if (!a.code) {
+            k = cut_key(tv[s], b);
+        } else {
+            s32 d = 0;
+            for (u32 t = 0; t <= mask; ++t) {
+                const u32 id = tk[t];
+                if (id != EMPTY) d = wadd(d, wmul(tv[t], wsub(D(a, o, id), D(a, b, id))));
+            }
+            k = delta_key(d, b);
+        }
+        bk = k > bk ? k : bk;
+    }
+    bk = Grp<BLK>::max_u64(bk, smu);
+    own = Grp<BLK>::sum_s64(own, sms);
+    if (Grp<BLK>::tid() == 0) {
+        if (!a.code) lp_finish_cut(a, u, (s32) own, bk, ratio);
+        else lp_finish_map(a, u, bk);
+    }
+    table_clear<BLK>(tk, tv, mask);
+}
+
+// Counts recomputed vertices / entries for roofline accounting.
+__device__ __forceinline__ void count_recompute(const JArgs &a, bool rec, u32 len) {
+    const unsigned mask = __ballot_sync(FULL, rec);
+    unsigned long long e = rec ? len : 0;
+    e = warp_sum<unsigned long long>(e);
+    if (lane_id() == 0 && mask) {
+        atomicAdd(&a.st->cnt[ST_AUX], (u32) __popc(mask));
+        atomicAdd((unsigned long long *) &a.st->sum[4], e);
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
+        const u32 u = (u32) (base + threadIdx.x);
+        int cls = 0;
+        u32 len = 0;
+        bool rec = false;
+        if (u < a.g.n) {
+            const u32 dc = a.dest_cache[u];
+            if (dc != NULL_PART) {
+                a.dest_part[u] = dc;
+            } else {
+                rec = true;
+                len = a.g.rowlen[u];
+                if (len <= JT) lp_thread(a, u, ratio);
+                else cls = len <= JW ? 1 : 2;
+            }
+        }
+        count_recompute(a, rec, len);
+        u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], cls == 1);
+        if (cls == 1) a.heavy[s1] = u;
+        u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
+        if (cls == 2) a.heavy2[s2] = u;
+    }
+}
+
+__global__ void __launch_bounds__(JW_BLOCK) k_lp_warp(JArgs a, u32 ratio) {
+    __shared__ u32 tk_all[JW_BLOCK / 32][JW_SLOTS];
+    __shared__ s32 tv_all[JW_BLOCK / 32][JW_SLOTS];
+    u32 *tk = tk_all[warp_in_block()];
+    s32 *tv = tv_all[warp_in_block()];
+    for (u32 s = lane_id(); s < JW_SLOTS; s += 32) {
+        tk[s] = EMPTY;
+        tv[s] = 0;
+    }
+    __syncwarp();
+    const u32 total = a.st->cnt[ST_HEAVY];
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const u32 u = a.heavy[i];
+        const u32 mask = table_mask_for(a.g.rowlen[u], a.k, JW_SLOTS);
+        lp_group<false>(a, u, ratio, tk, tv, mask, nullptr, nullptr);
+    }
+}
+
+__global__ void __launch_bounds__(JB_BLOCK) k_lp_block(JArgs a, u32 ratio) {
+    extern __shared__ u32 dsm[];
+    u32 *tk = dsm;
+    s32 *tv = (s32 *) (dsm + JB_SLOTS);
+    __shared__ unsigned long long smu[33];
+    __shared__ long long sms[33];
+    for (u32 s = threadIdx.x; s < JB_SLOTS; s += blockDim.x) {
+        tk[s] = EMPTY;
+        tv[s] = 0;
+    }
+    __syncthreads();
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
+        const u32 u = a.heavy2[i];
+        const u32 mask = table_mask_for(a.g.rowlen[u], a.k, JB_SLOTS);
+        lp_group<true>(a, u, ratio, tk, tv, mask, smu, sms);
+    }
+}
+
+// filter potentially viable moves (:247-258)
+__global__ void k_lp_filter(JArgs a) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
+        const u32 u = (u32) (base + threadIdx.x);
+        bool c = false;
+        if (u < a.g.n) {
+            c = a.dest_part[u] != NO_MOVE && a.lock[u] == 0;
+            if (c) {
+                a.gain1[u] = a.gain_cache[u];
+            } else {
+                a.gain1[u] = GAIN_MIN;
+                a.lock[u] = 0;
+            }
+        }
+        const u32 s = warp_append(&a.st->cnt[ST_CAND], c);
+        if (c) a.cand[s] = u;
+    }
+}
+
+// afterburner (:269-331 / ProMap :273-320): contribution of neighbour v.
+__device__ __forceinline__ s32 ab_term(const JArgs &a, u32 u, s32 ug, u32 ou, u32 nu, u32 v, s32 w) {
+    const s32 vg = a.gain1[v];
+    if (!(vg > ug || (vg == ug && v < u))) return 0;
+    const u32 nv = a.dest_part[v], ov = a.map[v];
+    if (!a.code) {
+        const s32 t = (s32) (nv == nu) - (s32) (nv == ou) + (s32) (ov == ou) - (s32) (ov == nu);
+        return wmul(w, t);
+    }
+    const s32 before_u = wsub(D(a, ou, ov), D(a, nu, ov));
+    const s32 after_u = wsub(D(a, ou, nv), D(a, nu, nv));
+    return wmul(w, wsub(after_u, before_u));
+}
+
+__global__ void k_ab_thread(JArgs a) {
+    const u32 total = a.st->cnt[ST_CAND];
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
+        const u64 i = base + threadIdx.x;
+        bool heavy = false, lock = false;
+        u32 u = 0;
+        if (i < total) {
+            u = a.cand[i];
+            const u32 len = a.g.rowlen[u];
+            if (len > AB_T) {
+                heavy = true;
+            } else {
+                const s32 ug = a.gain1[u];
+                const u32 ou = a.map[u], nu = a.dest_part[u];
+                const u64 beg = a.g.rowptr[u];
+                s32 change = 0;
+                for (u32 t = 0; t < len; ++t)
+                    change = wadd(change, ab_term(a, u, ug, ou, nu, a.g.adj[beg + t], g_ew(a.g, beg + t)));
+                if (wadd(ug, change) >= 0) {
+                    a.lock[u] = 1;
+                    lock = true;
+                }
+            }
+        }
+        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], heavy);
+        if (heavy) a.heavy[s1] = u;
+        const u32 s2 = warp_append(&a.st->cnt[ST_MOVES], lock);
+        if (lock) a.moves[s2] = u;
+    }
+}
+
+__global__ void k_ab_warp(JArgs a) {
+    const u32 total = a.st->cnt[ST_HEAVY];
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const u32 u = a.heavy[i];
+        const u32 len = a.g.rowlen[u];
+        const s32 ug = a.gain1[u];
+        const u32 ou = a.map[u], nu = a.dest_part[u];
+        const u64 beg = a.g.rowptr[u];
+        s32 change = 0;
+        for (u32 t = lane_id(); t < len; t += 32)
+            change = wadd(change, ab_term(a, u, ug, ou, nu, a.g.adj[beg + t], g_ew(a.g, beg + t)));
+        change = (s32) warp_sum<u32>((u32) change);
+        if (lane_id() == 0 && wadd(ug, change) >= 0) {
+            a.lock[u] = 1;
+            a.moves[atomicAdd(&a.st->cnt[ST_MOVES], 1u)] = u;
+        }
+    }
+}
+
+// ---- perform_moves (:753-924 / ProMap :1103-1216) -----------------------------------
+
+__global__ void k_mark_moving(JArgs a) {
+    const u32 total = a.st->cnt[ST_MOVES];
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const u32 u = a.moves[i];
+        if (a.dest_part[u] != a.map[u]) a.moving[u] = a.epoch;
+    }
+}
+
+__device__ __forceinline__ long long delta_term(const JArgs &a, u32 ou, u32 nu, u32 v, s32 w) {
+    const u32 ov = a.map[v];
+    const bool vm = a.moving[v] == a.epoch;
+    const u32 nv = vm ? a.dest_part[v] : ov;
+    long long c;
+    if (!a.code) c = (long long) w * ((long long) (nu != nv) - (long long) (ou != ov));
+    else c = (long long) w * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov));
+    return vm ? c : 2 * c;
+}
+
+__global__ void k_delta_thread(JArgs a) {
+    const u32 total = a.st->cnt[ST_MOVES];
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    long long acc = 0;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
+        const u64 i = base + threadIdx.x;
+        bool heavy = false;
+        u32 u = 0;
+        if (i < total) {
+            u = a.moves[i];
+            const u32 len = a.g.rowlen[u];
+            if (len > AB_T) {
+                heavy = true;
+            } else {
+                const u64 beg = a.g.rowptr[u];
+                const bool um = a.moving[u] == a.epoch;
+                const u32 ou = a.map[u], nu = a.dest_part[u];
+                for (u32 t = 0; t < len; ++t) {
+                    const u32 v = a.g.adj[beg + t];
+                    a.dest_cache[v] = NULL_PART;
+                    if (um) acc += delta_term(a, ou, nu, v, g_ew(a.g, beg + t));
+                }
+            }
+        }
+        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY2], heavy);
+        if (heavy) a.heavy2[s1] = u;
+    }
+    acc = warp_sum<long long>(acc);
+    if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
+}
+
+__global__ void k_delta_warp(JArgs a) {
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    long long acc = 0;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const u32 u = a.heavy2[i];
+        const u32 len = a.g.rowlen[u];
+        const u64 beg = a.g.rowptr[u];
+        const bool um = a.moving[u] == a.epoch;
+        const u32 ou = a.map[u], nu = a.dest_part[u];
+        for (u32 t = lane_id(); t < len; t += 32) {
+            const u32 v = a.g.adj[beg + t];
+            a.dest_cache[v] = NULL_PART;
+            if (um) acc += delta_term(a, ou, nu, v, g_ew(a.g, beg + t));
+        }
+    }
+    acc = warp_sum<long long>(acc);
+    if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
+}
+
+__global__ void k_apply(JArgs a) {
+    const u32 total = a.st->cnt[ST_MOVES];
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const u32 u = a.moves[i];
+        const u32 ou = a.map[u], nu = a.dest_part[u];
+        const s32 w = g_vw(a.g, u);
+        atomicSub(&a.bw[ou], w);
+        atomicAdd(&a.bw[nu], w);
+        a.map[u] = nu;
+        a.dest_part[u] = ou;
+        a.dest_cache[u] = NULL_PART;
+    }
+}
+
+__global__ void k_max_bw(const s32 *bw, u32 k, int *out) {
+    s32 m = 0;
+    for (u32 b = threadIdx.x; b < k; b += blockDim.x) m = bw[b] > m ? bw[b] : m;
+    m = __reduce_max_sync(FULL, m);
+    __shared__ s32 sm[32];
+    if (lane_id() == 0) sm[warp_in_block()] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s32 r = 0;
+        for (u32 w = 0; w < (blockDim.x >> 5); ++w) r = sm[w] > r ? sm[w] : r;
+        *out = r;
+    }
+}
+
+// ---- rebalancing (rebalance_weak :592-751, rebalance_strong :356-590) ----------------
+
+struct RbArgs {
+    s32 opt;
+    s32 max_b_w;
+    u32 sections;
+    const u32 *under;
+    u32 *keys;  // per vertex: mini-bucket key or NOKEY
+};
+
+// weak: best non-overloaded block by connection (:645-687)
+__device__ __forceinline__ void weak_finish(const JArgs &a, const RbArgs &r, u32 u, u32 o, s32 own,
+                                            unsigned long long bk) {
+    const u32 n_under = a.st->cnt[ST_AUX];
+    u32 best = o;
+    s32 gain = 0;
+    const s32 best_w = bk ? (s32) (u32) (bk >> 32) : 0;
+    if (best_w <= 0) {
+        if (n_under > 0) best = r.under[u % n_under];
+        gain = -own;
+    } else {
+        best = ~(u32) bk;
+        gain = wsub(best_w, own);
+    }
+    a.dest_part[u] = best;
+    const s32 vw = g_vw(a.g, u);
+    r.keys[u] = (o != best) ? (MAX_BUCKETS * o + gain_bucket(gain, vw)) * r.sections + (u % r.sections) : NOKEY;
+}
+
+// strong: average connection to non-full blocks minus own (:404-442)
+__device__ __forceinline__ void strong_finish(const JArgs &a, const RbArgs &r, u32 u, u32 o, s32 own, s32 sum,
+                                              s32 count) {
+    if (count == 0) count = 1;
+    const s32 gain = wsub(sum / count, own);
+    const s32 vw = g_vw(a.g, u);
+    const s32 excess = a.bw[o] - a.lmax;
+    r.keys[u] = (MAX_BUCKETS * o + gain_bucket(gain, vw < excess ? vw : excess)) * r.sections + (u % r.sections) + 1;
+}
+
+template<bool STRONG>
+__device__ __forceinline__ bool rb_qualifies(const JArgs &a, const RbArgs &r, u32 o, s32 vw, s32 maxv) {
+    const s64 ow = a.bw[o];
+    if (ow <= a.lmax) return false;
+    if (!STRONG) return 2 * (s64) vw < 3 * (ow - r.opt);
+    return (s64) vw <= 2 * (s64) maxv && (s64) vw < 2 * (ow - r.opt);
+}
+
+template<bool STRONG>
+__device__ __forceinline__ void rb_thread(const JArgs &a, const RbArgs &r, u32 u, u32 o) {
+    TRow row;
+    trow_build(a, u, row);
+    s32 own = 0, sum = 0, count = 0;
+    unsigned long long bk = 0;
+#pragma unroll
+    for (int s = 0; s < (int) JT; ++s) {
+        const u32 b = row.b[s];
+        if (b == EMPTY) continue;
+        if (b == o) {
+            own = row.c[s];
+            continue;
+        }
+        if (a.bw[b] < r.max_b_w) {
+            if (STRONG) {
+                sum = wadd(sum, row.c[s]);
+                ++count;
+            } else {
+                unsigned long long k = cut_key(row.c[s], b);
+                bk = k > bk ? k : bk;
+            }
+        }
+    }
+    if (STRONG) strong_finish(a, r, u, o, own, sum, count);
+    else weak_finish(a, r, u, o, own, bk);
+}
+
+template<bool STRONG, bool BLK>
+__device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u, u32 *tk, s32 *tv, u32 mask,
+                                         unsigned long long *smu, long long *sms) {
+    table_build<BLK>(a, u, tk, tv, mask);
+    const u32 o = a.map[u];
+    long long own = 0, sum = 0, count = 0;
+    unsigned long long bk = 0;
+    for (u32 s = Grp<BLK>::tid(); s <= mask; s += Grp<BLK>::size()) {
+        const u32 b = tk[s];
+        if (b == EMPTY) continue;
+        if (b == o) {
+            own = tv[s];
+            continue;
+        }
+        if (a.bw[b] < r.max_b_w) {
+            if (STRONG) {
+                sum = (long long) wadd((s32) sum, tv[s]);
+                ++count;
+            } else {
+                unsigned long long k = cut_key(tv[s], b);
+                bk = k > bk ? k : bk;
+            }
+        }
+    }
+    own = Grp<BLK>::sum_s64(own, sms);
+    if (STRONG) {
+        // s32 wrap-around sum: reduce the low 32 bits
+        sum = (long long) (s32) (u32) (unsigned long long) Grp<BLK>::sum_s64((long long) (u32) (s32) sum, sms);
+        count = Grp<BLK>::sum_s64(count, sms);
+    } else {
+        bk = Grp<BLK>::max_u64(bk, smu);
+    }
+    if (Grp<BLK>::tid() == 0) {
+        if (STRONG) strong_finish(a, r, u, o, (s32) own, (s32) sum, (s32) count);
+        else weak_finish(a, r, u, o, (s32) own, bk);
+    }
+    table_clear<BLK>(tk, tv, mask);
+}
+
+template<bool STRONG>
+__global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
+    const s32 maxv = a.st->imax[1];
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
+        const u32 u = (u32) (base + threadIdx.x);
+        int cls = 0;
+        if (u < a.g.n) {
+            const u32 o = a.map[u];
+            if (!rb_qualifies<STRONG>(a, r, o, g_vw(a.g, u), maxv)) {
+                if (!STRONG) a.dest_part[u] = o;
+                r.keys[u] = NOKEY;
+            } else {
+                const u32 len = a.g.rowlen[u];
+                if (len <= JT) rb_thread<STRONG>(a, r, u, o);
+                else cls = len <= JW ? 1 : 2;
+            }
+        }
+        u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], cls == 1);
+        if (cls == 1) a.heavy[s1] = u;
+        u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
+        if (cls == 2) a.heavy2[s2] = u;
+    }
+}
+
+template<bool STRONG>
+__global__ void __launch_bounds__(JW_BLOCK) k_rb_warp(JArgs a, RbArgs r) {
+    __shared__ u32 tk_all[JW_BLOCK / 32][JW_SLOTS];
+    __shared__ s32 tv_all[JW_BLOCK / 32][JW_SLOTS];
+    u32 *tk = tk_all[warp_in_block()];
+    s32 *tv = tv_all[warp_in_block()];
+    for (u32 s = lane_id(); s < JW_SLOTS; s += 32) {
+        tk[s] = EMPTY;
+        tv[s] = 0;
+    }
+    __syncwarp();
+    const u32 total = a.st->cnt[ST_HEAVY];
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const u32 u = a.heavy[i];
+        rb_group<STRONG, false>(a, r, u, tk, tv, table_mask_for(a.g.rowlen[u], a.k, JW_SLOTS), nullptr, nullptr);
+    }
+}
+
+template<bool STRONG>
+__global__ void __launch_bounds__(JB_BLOCK) k_rb_block(JArgs a, RbArgs r) {
+    extern __shared__ u32 dsm[];
+    u32 *tk = dsm;
+    s32 *tv = (s32 *) (dsm + JB_SLOTS);
+    __shared__ unsigned long long smu[33];
+    __shared__ long long sms[33];
+    for (u32 s = threadIdx.x; s < JB_SLOTS; s += blockDim.x) {
+        tk[s] = EMPTY;
+        tv[s] = 0;
+    }
+    __syncthreads();
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
+        const u32 u = a.heavy2[i];
+        rb_group<STRONG, true>(a, r, u, tk, tv, table_mask_for(a.g.rowlen[u], a.k, JB_SLOTS), smu, sms);
+    }
+}
+
+// underloaded_blocks (:614-627): ordered list of blocks below max_b_w.
+__global__ void k_under(const s32 *bw, u32 k, s32 max_b_w, u32 *under, u32 *n_under) {
+    __shared__ u32 sm[32];
+    u32 carry = 0;
+    for (u32 base = 0; base < k; base += blockDim.x) {
+        const u32 b = base + threadIdx.x;
+        const u32 f = (b < k && bw[b] < max_b_w) ? 1u : 0u;
+        u32 tot;
+        const u32 p = block_exclusive_scan<u32>(f, tot, sm);
+        if (f) under[carry + p] = b;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) *n_under = carry;
+}
+
+// find max size (:377-385): largest free capacity below max_b_w (INT32_MIN if none)
+__global__ void k_maxv(const s32 *bw, u32 k, s32 max_b_w, int *out) {
+    s32 m = INT32_MIN;
+    for (u32 b = threadIdx.x; b < k; b += blockDim.x)
+        if (bw[b] < max_b_w && max_b_w - bw[b] > m) m = max_b_w - bw[b];
+    m = __reduce_max_sync(FULL, m);
+    __shared__ s32 sm[32];
+    if (lane_id() == 0) sm[warp_in_block()] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s32 r = INT32_MIN;
+        for (u32 w = 0; w < (blockDim.x >> 5); ++w) r = sm[w] > r ? sm[w] : r;
+        *out = r;
+    }
+}
+
+// B(x) for x = p * width, p in [0, k]: weight of candidates with key < x.
+__global__ void k_bounds(const u32 *skeys, const long long *prefix, u32 c, u32 k, u32 width, long long *B) {
+    for (u32 p = blockIdx.x * blockDim.x + threadIdx.x; p <= k; p += gridDim.x * blockDim.x) {
+        const u64 x = (u64) p * width;
+        u32 lo = 0, hi = c;
+        while (lo < hi) {
+            const u32 mid = (lo + hi) >> 1;
+            if ((u64) skeys[mid] < x) lo = mid + 1;
+            else hi = mid;
+        }
+        B[p] = prefix[lo];
+    }
+}
+
+__global__ void k_weak_filter(JArgs a, const u32 *svals, const long long *prefix, const long long *B, u32 c) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < c; base += stride) {
+        const u64 i = base + threadIdx.x;
+        bool take = false;
+        u32 u = 0;
+        if (i < c) {
+            u = svals[i];
+            const u32 o = a.map[u];
+            const long long score = prefix[i] - B[o];
+            take = score < (long long) a.bw[o] - a.lmax;
+        }
+        const u32 s = warp_append(&a.st->cnt[ST_MOVES], take);
+        if (take) a.moves[s] = u;
+    }
+}
+
+__global__ void k_strong_filter(JArgs a, const u32 *svals, const long long *prefix, const long long *B, u32 c,
+                                long long *evict_adjust, long long *mpre) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < c; base += stride) {
+        const u64 i = base + threadIdx.x;
+        bool take = false;
+        u32 u = 0;
+        if (i < c) {
+            u = svals[i];
+            const u32 o = a.map[u];
+            const long long score = prefix[i] - B[o];
+            const long long limit = (long long) a.bw[o] - a.lmax;
+            if (score < limit) {
+                take = true;
+                const long long vw = g_vw(a.g, u);
+                if (score + vw >= limit) evict_adjust[o] = score + vw;
+            }
+        }
+        const u32 s = warp_append(&a.st->cnt[ST_MOVES], take);
+        if (take) {
+            a.moves[s] = u;
+            mpre[s] = prefix[i];
+        }
+    }
+}
+
+// cookie cutter (:524-551)
+__global__ void k_cookie(const s32 *bw, u32 k, s32 max_b_w, const long long *B, long long *ea, long long *es,
+                         long long *max_v) {
+    __shared__ long long sm[32];
+    long long carry = 0, carry2 = 0;
+    for (u32 base = 0; base < k; base += blockDim.x) {
+        const u32 p = base + threadIdx.x;
+        long long add = 0, cap = 0;
+        if (p < k) {
+            add = ea[p];
+            if (add == 0) add = B[p + 1] - B[p];
+            cap = max_b_w > bw[p] ? (long long) max_b_w - bw[p] : 0;
+        }
+        long long tot, tot2;
+        const long long pa = block_exclusive_scan<long long>(add, tot, sm);
+        const long long pc = block_exclusive_scan<long long>(cap, tot2, sm);
+        if (p < k) {
+            ea[p] = B[p] - (carry + pa);
+            es[p + 1] = carry2 + pc + cap;
+        }
+        carry += tot;
+        carry2 += tot2;
+    }
+    if (threadIdx.x == 0) {
+        es[0] = 0;
+        *max_v = carry;
+    }
+}
+
+__device__ __forceinline__ s32 chunk_of(const long long *es, u32 k, long long tg) {
+    // largest id in [0, k] with es[id] <= tg (es non-decreasing, es[0] = 0)
+    u32 lo = 0, hi = k + 1;
+    while (lo < hi) {
+        const u32 mid = (lo + hi) >> 1;
+        if (es[mid] <= tg) lo = mid + 1;
+        else hi = mid;
+    }
+    return (s32) lo - 1;
+}
+
+// adjust_scores (:560-584): first attempt for every evicted vertex; those
+// that need a fallback slot are collected.
+__global__ void k_strong_assign(JArgs a, const long long *mpre, const long long *ea, const long long *es, u32 *fail,
+                                u32 *n_fail) {
+    const u32 total = a.st->cnt[ST_MOVES];
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
+        const u64 j = base + threadIdx.x;
+        bool f = false;
+        u32 u = 0;
+        if (j < total) {
+            u = a.moves[j];
+            const u32 o = a.map[u];
+            const long long vw = g_vw(a.g, u);
+            const long long tg = mpre[j] - ea[o];
+            const s32 id = chunk_of(es, a.k, tg);
+            if (id < (s32) a.k && vw / 2 <= es[id + 1] - tg) {
+                a.dest_part[u] = (u32) id;
+            } else {
+                a.dest_part[u] = o;
+                f = id < (s32) a.k;
+            }
+        }
+        const u32 s = warp_append(n_fail, f);
+        if (f) fail[s] = u;
+    }
+}
+
+// Fallback slots in ascending vertex order (one thread; at most one
+// straddling vertex per chunk boundary reaches this).
+__global__ void k_strong_fallback(JArgs a, const u32 *fail, u32 nf, const long long *es, long long *max_v) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long mv = *max_v;
+    for (u32 i = 0; i < nf; ++i) {
+        const u32 u = fail[i];
+        const u32 o = a.map[u];
+        const long long vw = g_vw(a.g, u);
+        u32 dest = o;
+        for (u32 guard = 0; guard < 2 * a.k + 4; ++guard) {
+            const long long tg = mv;
+            mv += vw;
+            const s32 id = chunk_of(es, a.k, tg);
+            if (id >= (s32) a.k) break;
+            if (vw / 2 <= es[id + 1] - tg) {
+                dest = (u32) id;
+                break;
+            }
+        }
+        a.dest_part[u] = dest;
+    }
+    *max_v = mv;
+}
+
+// ---- objectives ------------------------------------------------------------------
+
+__global__ void k_objective(DGraph g, const u32 *part, const u32 *code, const s32 *bitdist, unsigned long long *out) {
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    long long acc = 0;
+    for (u32 u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < g.n; u += warps) {
+        const u64 beg = g.rowptr[u];
+        const u32 len = g.rowlen[u];
+        const u32 pu = part[u];
+        for (u32 t = lane_id(); t < len; t += 32) {
+            const u32 pv = part[g.adj[beg + t]];
+            const long long w = g_ew(g, beg + t);
+            if (code) acc += w * dist_of(code, bitdist, pu, pv);
+            else acc += pu != pv ? w : 0;
+        }
+    }
+    acc = warp_sum<long long>(acc);
+    if (lane_id() == 0 && acc) atomicAdd(out, (unsigned long long) acc);
+}
+
+__global__ void k_block_weights(DGraph g, const u32 *part, s32 *bw) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < g.n; u += gridDim.x * blockDim.x)
+        atomicAdd(&bw[part[u]], g_vw(g, u));
+}
+
+JArgs make_args(JetLevel &L) {
+    JArgs a;
+    a.g = L.g;
+    a.k = L.k;
+    a.lmax = L.lmax;
+    a.g_weight = L.g_weight;
+    a.code = L.D ? L.D->code : nullptr;
+    a.bitdist = L.D ? L.D->bitdist : nullptr;
+    a.map = L.map;
+    a.bw = L.bw;
+    a.dest_cache = L.dest_cache;
+    a.gain_cache = L.gain_cache;
+    a.lock = L.lock;
+    a.dest_part = L.dest_part;
+    a.gain1 = L.gain1;
+    a.moving = L.moving;
+    a.epoch = L.epoch;
+    a.cand = L.cand;
+    a.moves = L.moves;
+    a.heavy = L.heavy;
+    a.heavy2 = L.heavy2;
+    a.st = L.ctx->d_status;
+    return a;
+}
+
+void sections_of(u32 n, u32 k, u32 &sections, u32 &width) {
+    sections = MAX_SECTIONS;
+    u32 section_size = (n + sections * k) / (sections * k);
+    if (section_size < 4096) {
+        section_size = 4096;
+        sections = (n + section_size * k) / (section_size * k);
+    }
+    width = MAX_BUCKETS * sections;
+}
+
+void set_big_smem() {
+    static bool done = false;
+    if (done) return;
+    const int smem = (int) (JB_SLOTS * 8);
+    HP_CUDA(cudaFuncSetAttribute(k_lp_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    HP_CUDA(cudaFuncSetAttribute(k_rb_block<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    HP_CUDA(cudaFuncSetAttribute(k_rb_block<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    done = true;
+}
+
+} // namespace
+
+// ---- distance oracle -----------------------------------------------------------------
+
+DistOracle make_dist_oracle(Ctx &ctx, const std::vector<u32> &hier, const std::vector<s32> &dist) {
+    DistOracle D;
+    D.hier = hier;
+    D.dist = dist;
+    const u32 l = (u32) hier.size();
+    if (l == 0 || dist.size() != l) throw HpError{HP_ERR_ARG, "hierarchy and distance must have the same length"};
+    u64 k = 1;
+    std::vector<u32> bits(l), off(l);
+    u32 total = 0;
+    for (u32 t = 0; t < l; ++t) {
+        if (hier[t] == 0) throw HpError{HP_ERR_ARG, "hierarchy entries must be positive"};
+        k *= hier[t];
+        u32 b = 0;
+        while ((1ull << b) < hier[t]) ++b;
+        bits[t] = b;
+        off[t] = total;
+        total += b;
+    }
+    if (k > MAX_K || total > 32) throw HpError{HP_ERR_ARG, "hierarchy too large"};
+    D.k = (u32) k;
+    std::vector<u32> code(k);
+    for (u32 i = 0; i < k; ++i) {
+        u32 x = i, c = 0;
+        for (u32 t = 0; t < l; ++t) {
+            c |= (x % hier[t]) << off[t];
+            x /= hier[t];
+        }
+        code[i] = c;
+    }
+    std::vector<s32> bd(32, 0);
+    for (u32 t = 0; t < l; ++t)
+        for (u32 b = 0; b < bits[t]; ++b) bd[off[t] + b] = dist[t];
+    D.code = ctx.falloc<u32>(k);
+    D.bitdist = ctx.falloc<s32>(32);
+    HP_CUDA(cudaMemcpyAsync(D.code, code.data(), sizeof(u32) * k, cudaMemcpyHostToDevice, ctx.stream));
+    HP_CUDA(cudaMemcpyAsync(D.bitdist, bd.data(), sizeof(s32) * 32, cudaMemcpyHostToDevice, ctx.stream));
+    ctx.sync();  // host vectors go out of scope
+    return D;
+}
+
+s64 edge_cut_dev(Ctx &ctx, const DGraph &g, const u32 *part) {
+    ctx.zero_counters();
+    k_objective<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(
+        g, part, nullptr, nullptr, (unsigned long long *) &ctx.d_status->sum[0]);
+    HP_LAUNCH_CHECK();
+    return ctx.read_status().sum[0] / 2;
+}
+
+s64 comm_cost_dev(Ctx &ctx, const DGraph &g, const u32 *part, const DistOracle &D) {
+    ctx.zero_counters();
+    k_objective<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(
+        g, part, D.code, D.bitdist, (unsigned long long *) &ctx.d_status->sum[0]);
+    HP_LAUNCH_CHECK();
+    return ctx.read_status().sum[0];
+}
+
+void block_weights(Ctx &ctx, const DGraph &g, const u32 *part, u32 k, s32 *bw) {
+    HP_CUDA(cudaMemsetAsync(bw, 0, sizeof(s32) * k, ctx.stream));
+    k_block_weights<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, bw);
+    HP_LAUNCH_CHECK();
+}
+
+s32 max_block_weight(Ctx &ctx, const s32 *bw, u32 k) {
+    ctx.zero_counters();
+    k_max_bw<<<1, 1024, 0, ctx.stream>>>(bw, k, &ctx.d_status->imax[MAX_BW]);
+    HP_LAUNCH_CHECK();
+    return ctx.read_status().imax[MAX_BW];
+}
+
+// ---- JetLevel -----------------------------------------------------------------------
+
+void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle *d, const u32 *part) {
+    ctx = &c;
+    g = gr;
+    k = kk;
+    lmax = lm;
+    D = d;
+    g_weight = (s32) gr.total_vw;
+    const u32 n = g.n;
+    map = c.balloc<u32>(n);
+    bw = c.balloc<s32>(k);
+    dest_cache = c.balloc<u32>(n);
+    gain_cache = c.balloc<s32>(n);
+    lock = c.balloc<u32>(n);
+    dest_part = c.balloc<u32>(n);
+    gain1 = c.balloc<s32>(n);
+    moving = c.balloc<u32>(n);
+    cand = c.balloc<u32>(n);
+    moves = c.balloc<u32>(n);
+    heavy = c.balloc<u32>(n);
+    heavy2 = c.balloc<u32>(n);
+    epoch = 0;
+    HP_CUDA(cudaMemcpyAsync(map, part, sizeof(u32) * n, cudaMemcpyDeviceToDevice, c.stream));
+    device_fill<u32>(c, dest_cache, n, NULL_PART);
+    HP_CUDA(cudaMemsetAsync(gain_cache, 0, sizeof(s32) * n, c.stream));
+    HP_CUDA(cudaMemsetAsync(lock, 0, sizeof(u32) * n, c.stream));
+    HP_CUDA(cudaMemsetAsync(moving, 0, sizeof(u32) * n, c.stream));
+    device_fill<u32>(c, dest_part, n, NO_MOVE);
+    HP_CUDA(cudaMemsetAsync(gain1, 0, sizeof(s32) * n, c.stream));
+    block_weights(c, g, map, k, bw);
+    set_big_smem();
+}
+
+void JetLevel::gain_pass(u32 ratio_pct) {
+    Ctx &c = *ctx;
+    JArgs a = make_args(*this);
+    const u32 n = g.n;
+    c.instr.begin(c.stream, "jet_gain", 0.0);
+    k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct);
+    k_lp_warp<<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, ratio_pct);
+    k_lp_block<<<c.sm_count, JB_BLOCK, JB_SLOTS * 8, c.stream>>>(a, ratio_pct);
+    HP_LAUNCH_CHECK();
+    c.instr.end(c.stream);
+}
+
+void JetLevel::lp(u32 ratio_pct) {
+    Ctx &c = *ctx;
+    c.zero_counters();
+    gain_pass(ratio_pct);
+    JArgs a = make_args(*this);
+    const u32 n = g.n;
+    k_lp_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
+    k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+    k_ab_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+    HP_LAUNCH_CHECK();
+}
+
+void JetLevel::weak() {
+    Ctx &c = *ctx;
+    const u32 n = g.n;
+    const s32 opt = (g_weight + (s32) (k - 1)) / (s32) k;
+    s32 max_b_w = (s32) ((99 * (s64) lmax) / 100);
+    if (max_b_w < lmax - 100) max_b_w = lmax - 100;
+    u32 sections, width;
+    sections_of(n, k, sections, width);
+    ScratchScope ss(c.arena);
+    u32 *under = c.balloc<u32>(k);
+    u32 *keys = c.balloc<u32>(n);
+    c.zero_counters();
+    k_under<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, under, &c.d_status->cnt[ST_AUX]);
+    JArgs a = make_args(*this);
+    RbArgs r{opt, max_b_w, sections, under, keys};
+    k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r);
+    k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r);
+    k_rb_block<false><<<c.sm_count, JB_BLOCK, JB_SLOTS * 8, c.stream>>>(a, r);
+    HP_LAUNCH_CHECK();
+    // ordered candidates (ascending id), then a stable sort by mini-bucket key
+    u32 *cands = c.balloc<u32>(n);
+    u32 *ck = c.balloc<u32>(n);
+    device_scan<u32>(
+        c, n, [=] __device__(u64 i) -> u32 { return keys[i] != NOKEY ? 1u : 0u; },
+        [=] __device__(u64 i, u32 p, u32 v) {
+            if (v) {
+                cands[p] = (u32) i;
+                ck[p] = keys[i];
+            }
+        },
+        &c.d_status->cnt[ST_CAND]);
+    const u32 cc = c.read_status().cnt[ST_CAND];
+    radix_sort_pairs<u32>(c, ck, cands, cc, 0, bits_for((u64) MAX_BUCKETS * k * sections + 1));
+    long long *prefix = c.balloc<long long>((u64) cc + 1);
+    const DGraph gg = g;
+    device_scan<long long>(
+        c, (u64) cc + 1, [=] __device__(u64 i) -> long long { return i < cc ? (long long) g_vw(gg, cands[i]) : 0; },
+        [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr);
+    long long *B = c.balloc<long long>((u64) k + 1);
+    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B);
+    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_MOVES], 0, sizeof(u32), c.stream));
+    k_weak_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc);
+    HP_LAUNCH_CHECK();
+}
+
+void JetLevel::strong() {
+    Ctx &c = *ctx;
+    const u32 n = g.n;
+    const s32 opt = (g_weight + (s32) (k - 1)) / (s32) k;
+    const s32 max_b_w = std::max<s32>(opt + 1, (s32) ((99 * (s64) lmax) / 100));
+    u32 sections, width;
+    sections_of(n, k, sections, width);
+    ScratchScope ss(c.arena);
+    u32 *keys = c.balloc<u32>(n);
+    c.zero_counters();
+    k_maxv<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, &c.d_status->imax[1]);
+    JArgs a = make_args(*this);
+    RbArgs r{opt, max_b_w, sections, nullptr, keys};
+    k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r);
+    k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r);
+    k_rb_block<true><<<c.sm_count, JB_BLOCK, JB_SLOTS * 8, c.stream>>>(a, r);
+    HP_LAUNCH_CHECK();
+    u32 *cands = c.balloc<u32>(n);
+    u32 *ck = c.balloc<u32>(n);
+    device_scan<u32>(
+        c, n, [=] __device__(u64 i) -> u32 { return keys[i] != NOKEY ? 1u : 0u; },
+        [=] __device__(u64 i, u32 p, u32 v) {
+            if (v) {
+                cands[p] = (u32) i;
+                ck[p] = keys[i];
+            }
+        },
+        &c.d_status->cnt[ST_CAND]);
+    const u32 cc = c.read_status().cnt[ST_CAND];
+    radix_sort_pairs<u32>(c, ck, cands, cc, 0, bits_for((u64) MAX_BUCKETS * k * sections + 2));
+    long long *prefix = c.balloc<long long>((u64) cc + 1);
+    const DGraph gg = g;
+    device_scan<long long>(
+        c, (u64) cc + 1, [=] __device__(u64 i) -> long long { return i < cc ? (long long) g_vw(gg, cands[i]) : 0; },
+        [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr);
+    long long *B = c.balloc<long long>((u64) k + 1);
+    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B);
+    long long *ea = c.balloc<long long>(k);
+    long long *es = c.balloc<long long>((u64) k + 1);
+    long long *mpre = c.balloc<long long>((u64) cc + 1);
+    HP_CUDA(cudaMemsetAsync(ea, 0, sizeof(long long) * k, c.stream));
+    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_MOVES], 0, sizeof(u32), c.stream));
+    k_strong_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc, ea, mpre);
+    long long *max_v = (long long *) &c.d_status->sum[3];
+    k_cookie<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, B, ea, es, max_v);
+    u32 *fail = c.balloc<u32>(n);
+    u32 *n_fail = &c.d_status->cnt[ST_HEAVY];
+    HP_CUDA(cudaMemsetAsync(n_fail, 0, sizeof(u32), c.stream));
+    k_strong_assign<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, mpre, ea, es, fail, n_fail);
+    HP_LAUNCH_CHECK();
+    const u32 nf = c.read_status().cnt[ST_HEAVY];
+    if (nf) {
+        u32 *fk = c.balloc<u32>(nf);
+        HP_CUDA(cudaMemcpyAsync(fk, fail, sizeof(u32) * nf, cudaMemcpyDeviceToDevice, c.stream));
+        radix_sort_pairs<u32>(c, fk, fail, nf, 0, 32);
+        k_strong_fallback<<<1, 32, 0, c.stream>>>(a, fail, nf, es, max_v);
+        HP_LAUNCH_CHECK();
+    }
+}
+
+void JetLevel::perform() {
+    Ctx &c = *ctx;
+    ++epoch;
+    JArgs a = make_args(*this);
+    const u32 n = g.n;
+    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
+    HP_CUDA(cudaMemsetAsync(&c.d_status->sum[SUM_DELTA], 0, sizeof(long long), c.stream));
+    k_mark_moving<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+    k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+    k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+    k_apply<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+    k_max_bw<<<1, 1024, 0, c.stream>>>(bw, k, &c.d_status->imax[MAX_BW]);
+    HP_LAUNCH_CHECK();
+}
+
+void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultra, u32 level, s64 &obj, s32 &maxw,
+                const DistOracle *D) {
+    if (g.n == 0 || k <= 1) return;
+    ScratchScope ss(ctx.arena);
+    JetLevel L;
+    L.setup(ctx, g, k, lmax, D, part);
+    const bool promap = D != nullptr;
+    s64 best_obj = obj;
+    s32 best_max = maxw;
+    std::vector<u32> ratios;
+    if (ultra && !promap) ratios = {85, 80, 75, 70, 65, 60, 55, 50, 45, 40, 35, 30, 25, 20, 15, 10, 5};
+    else ratios = {level == 0 ? 25u : 75u};
+    for (u32 ratio: ratios) {
+        u32 balance_iteration = 0, iteration = 0;
+        while (iteration < JET_MAX_ITERATIONS) {
+            iteration += 1;
+            bool lp_iter = false;
+            if (!promap) {
+                if (maxw <= lmax) {
+                    L.lp(ratio);
+                    lp_iter = true;
+                    balance_iteration = 0;
+                } else if (balance_iteration < JET_MAX_WEAK_ITERATIONS) {
+                    L.weak();
+                } else {
+                    L.strong();
+                }
+            } else {
+                if (maxw <= lmax) {
+                    L.lp(ratio);
+                    lp_iter = true;
+                    balance_iteration = 0;
+                } else {
+                    balance_iteration++;
+                    if (balance_iteration < JET_MAX_WEAK_ITERATIONS) L.weak();
+                    else L.strong();
+                }
+            }
+            L.perform();
+            const DevStatus &st = ctx.read_status();
+            if (st.err) throw HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
+            const u32 nm = st.cnt[ST_MOVES];
+            if (!promap) {
+                if (nm == 0) {
+                    if (lp_iter) break;
+                    if (balance_iteration < JET_MAX_WEAK_ITERATIONS) {
+                        balance_iteration = JET_MAX_WEAK_ITERATIONS;
+                        continue;
+                    }
+                    break;
+                }
+                if (!lp_iter) balance_iteration++;
+            } else if (nm == 0) {
+                continue;
+            }
+            const s64 d = st.sum[SUM_DELTA];
+            obj += promap ? d : d / 2;
+            maxw = st.imax[MAX_BW];
+            const bool leq = promap ? (maxw < best_max) : (maxw <= best_max);
+            if (best_max > lmax && maxw < best_max) {
+                HP_CUDA(cudaMemcpyAsync(part, L.map, sizeof(u32) * g.n, cudaMemcpyDeviceToDevice, ctx.stream));
+                best_obj = obj;
+                best_max = maxw;
+                iteration = 0;
+            } else if (obj < best_obj && (maxw <= lmax || leq)) {
+                if (1000 * obj < 999 * best_obj) iteration = 0;  // PHI = 0.999
+                HP_CUDA(cudaMemcpyAsync(part, L.map, sizeof(u32) * g.n, cudaMemcpyDeviceToDevice, ctx.stream));
+                best_obj = obj;
+                best_max = maxw;
+            }
+        }
+    }
+    obj = best_obj;
+    maxw = best_max;
+    ctx.sync();
+}
+
+} // namespace hp

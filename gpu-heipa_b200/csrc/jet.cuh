@@ -1,0 +1,98 @@
+// Jet label-propagation refinement on the device for the edge cut
+// (src/refinement/jet_label_propagation.h) and for the process-mapping
+// objective J(C,D,Pi) (src/refinement/promap_jet_label_propagation.h).
+//
+// Connectivity rows are not stored: every pass that needs conn(u, b) for a
+// vertex aggregates it on the fly from the CSR row and the current labels
+// (registers for degree <= 16, a per-warp shared-memory hash table for
+// degree <= 512, a per-block table beyond). The dest/gain cache of the
+// reference (dest_cache/gain_cache, invalidated when the vertex or one of its
+// neighbours moves) is kept, so a pass only reaches vertices whose
+// neighbourhood changed.
+#pragma once
+#include "graph.cuh"
+
+namespace hp {
+
+// Hierarchy distance oracle computed from label digits instead of a k x k
+// matrix (src/distance_oracles/distance_oracle_matrix.h:64-99): every block id
+// gets a code with its mixed-radix digits packed low digit first; the
+// distance of two different blocks is distance[level of the highest
+// differing digit].
+struct DistOracle {
+    u32 k = 0;
+    std::vector<u32> hier;
+    std::vector<s32> dist;
+    u32 *code = nullptr;     // device, k entries
+    s32 *bitdist = nullptr;  // device, 32 entries: distance by highest differing bit
+};
+
+DistOracle make_dist_oracle(Ctx &ctx, const std::vector<u32> &hier, const std::vector<s32> &dist);
+
+__device__ __forceinline__ s32 dist_of(const u32 *code, const s32 *bitdist, u32 a, u32 b) {
+    if (a == b) return 0;
+    const u32 x = __ldg(&code[a]) ^ __ldg(&code[b]);
+    return __ldg(&bitdist[31 - __clz(x)]);
+}
+
+// Objectives (int64): edge_cut.h:71-90 (halved) and comm_cost.h:36-56 (not).
+s64 edge_cut_dev(Ctx &ctx, const DGraph &g, const u32 *part);
+s64 comm_cost_dev(Ctx &ctx, const DGraph &g, const u32 *part, const DistOracle &D);
+
+// Block weights of a labelling (partition.h:107-123) and their maximum.
+void block_weights(Ctx &ctx, const DGraph &g, const u32 *part, u32 k, s32 *bw);
+s32 max_block_weight(Ctx &ctx, const s32 *bw, u32 k);
+
+// Per-level Jet state (device arrays from the arena's back end).
+struct JetLevel {
+    Ctx *ctx = nullptr;
+    DGraph g;
+    u32 k = 0;
+    s32 lmax = 0;
+    s32 g_weight = 0;
+    const DistOracle *D = nullptr;  // null: edge cut
+    u32 *map = nullptr;
+    s32 *bw = nullptr;
+    u32 *dest_cache = nullptr;
+    s32 *gain_cache = nullptr;
+    u32 *lock = nullptr;
+    u32 *dest_part = nullptr;
+    s32 *gain1 = nullptr;
+    u32 *moving = nullptr;  // epoch stamps of vertices moving in this iteration
+    u32 epoch = 0;
+    u32 *cand = nullptr;
+    u32 *moves = nullptr;
+    u32 *heavy = nullptr;
+    u32 *heavy2 = nullptr;
+
+    void setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle *d, const u32 *part);
+    // Each of these fills `moves` and leaves the move count in the status
+    // word's MOVES counter (no host synchronisation for lp()).
+    void lp(u32 ratio_pct);
+    void weak();
+    void strong();
+    // Applies the moves; leaves the objective delta and the new maximum block
+    // weight in the status word.
+    void perform();
+    // Single pass helpers used by tests: recompute gains for all vertices
+    // whose cache is invalid (the "Jet-gain" kernel).
+    void gain_pass(u32 ratio_pct);
+};
+
+// Status word slots used by Jet.
+constexpr int ST_MOVES = 3;
+constexpr int ST_HEAVY = 4;
+constexpr int ST_CAND = 5;
+constexpr int ST_HEAVY2 = 6;
+constexpr int ST_AUX = 7;
+constexpr int SUM_DELTA = 2;
+constexpr int MAX_BW = 0;
+
+// jet_refine (jet_label_propagation.h:926-1033) / ProMap_jet_refine
+// (promap_jet_label_propagation.h:1218-1311). `part` (device, g.n) holds the
+// input labelling and receives the best labelling found; obj / maxw are the
+// running objective (edge cut or J) and maximum block weight.
+void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultra, u32 level, s64 &obj, s32 &maxw,
+                const DistOracle *D);
+
+} // namespace hp

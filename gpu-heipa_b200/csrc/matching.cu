@@ -1,0 +1,405 @@
+// Two-hop heavy-edge matching on the device; the semantics follow
+// src/coarsening/two_hop_matching.h:93-650 with the deterministic commit and
+// grouping rules documented in coarsen.cuh.
+#include "coarsen.cuh"
+#include "prims.cuh"
+
+namespace hp {
+namespace {
+
+// Argmax over the eligible neighbours of u of (edge weight, xorshift(v + r)),
+// r = xorshift(u ^ seed): pick_neighbor_flat two_hop_matching.h:102-141.
+template<bool INITIAL>
+__device__ __forceinline__ u32 pick_thread(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed) {
+    const u32 r = xorshift32(u ^ seed);
+    const u64 beg = g.rowptr[u];
+    const u32 len = g.rowlen[u];
+    u32 h = SENTINEL, tbb = 0;
+    s32 maxw = 0;
+    for (u32 t = 0; t < len; ++t) {
+        const u32 v = g.adj[beg + t];
+        if (!INITIAL && vcmap[v] != SENTINEL) continue;
+        if (g.ew) {
+            const s32 w = g.ew[beg + t];
+            if (maxw < w) {
+                maxw = w;
+                h = v;
+                tbb = xorshift32(v + r);
+                continue;
+            }
+            if (maxw != w) continue;
+        }
+        const u32 tb = xorshift32(v + r);
+        if (tb >= tbb) {
+            h = v;
+            tbb = tb;
+        }
+    }
+    return h;
+}
+
+// Warp version of pick_thread (pick_neighbor_team :143-188 selects the same
+// vertex): lane-local argmax, then a two-step warp reduction.
+template<bool INITIAL>
+__device__ __forceinline__ u32 pick_warp(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed) {
+    const u32 r = xorshift32(u ^ seed);
+    const u64 beg = g.rowptr[u];
+    const u32 len = g.rowlen[u];
+    u32 h = SENTINEL, tbb = 0;
+    s32 maxw = 0;
+    bool found = false;
+    for (u32 t = lane_id(); t < len; t += 32) {
+        const u32 v = g.adj[beg + t];
+        if (!INITIAL && vcmap[v] != SENTINEL) continue;
+        const s32 w = g.ew ? g.ew[beg + t] : 0;
+        const u32 tb = xorshift32(v + r);
+        if (!found || w > maxw || (w == maxw && tb >= tbb)) {
+            maxw = w;
+            tbb = tb;
+            h = v;
+            found = true;
+        }
+    }
+    const s32 wbest = __reduce_max_sync(FULL, found ? maxw : INT32_MIN);
+    if (wbest == INT32_MIN) return SENTINEL;
+    const bool elig = found && maxw == wbest;
+    const u32 tbest = __reduce_max_sync(FULL, elig ? tbb : 0u);
+    const unsigned win = __ballot_sync(FULL, elig && tbb == tbest);
+    return __shfl_sync(FULL, h, __ffs(win) - 1);
+}
+
+__global__ void k_match_init(DGraph g, u32 *vcmap, u32 *hn, u32 seed, u32 *heavy, u32 *heavy_cnt) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < g.n; base += stride) {
+        const u32 u = (u32) (base + threadIdx.x);
+        bool is_heavy = false;
+        if (u < g.n) {
+            vcmap[u] = SENTINEL;
+            const u32 len = g.rowlen[u];
+            if (!g.ew) {
+                // initial_pick_uniform two_hop_matching.h:279-284
+                hn[u] = len ? g.adj[g.rowptr[u] + (xorshift32(u ^ seed) % len)] : SENTINEL;
+            } else if (len <= THREAD_DEG_MAX) {
+                hn[u] = pick_thread<true>(g, vcmap, u, seed);
+            } else {
+                hn[u] = SENTINEL;
+                is_heavy = true;
+            }
+        }
+        u32 slot = warp_append(heavy_cnt, is_heavy);
+        if (is_heavy) heavy[slot] = u;
+    }
+}
+
+template<bool INITIAL>
+__global__ void k_pick_heavy(DGraph g, const u32 *vcmap, u32 *hn, u32 seed, const u32 *list, const u32 *cnt) {
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    const u32 c = *cnt;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < c; i += warps) {
+        const u32 u = list[i];
+        const u32 h = pick_warp<INITIAL>(g, vcmap, u, seed);
+        if (lane_id() == 0) hn[u] = h;
+    }
+}
+
+__device__ __forceinline__ bool commit_cond(u32 u, u32 v, u32 r) {
+    return r > 0 ? (murmur3_u32(u + r) < murmur3_u32(v + r)) : (u < v);
+}
+
+// commit_p1 two_hop_matching.h:313-319: mark receivers.
+__global__ void k_mark(const u32 *list, u32 cnt, const u32 *hn, u32 *vcmap, u32 r) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const u32 u = list[i];
+        const u32 v = hn[u];
+        if (v == SENTINEL || vcmap[u] != SENTINEL) continue;
+        if (!commit_cond(u, v, r)) vcmap[u] = SENTINEL - 1;
+    }
+}
+
+// commit_p2 two_hop_matching.h:320-327, deterministic: every proposer whose
+// target is a receiver offers itself; the smallest offer of the current epoch
+// wins (tags decrease with the epoch so stale offers lose).
+__global__ void k_claim(const u32 *list, u32 cnt, const u32 *hn, const u32 *vcmap, unsigned long long *claim,
+                        u32 tag) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const u32 u = list[i];
+        const u32 v = hn[u];
+        if (v == SENTINEL || vcmap[u] != SENTINEL) continue;
+        if (vcmap[v] == SENTINEL - 1) atomicMin(&claim[v], ((unsigned long long) tag << 32) | u);
+    }
+}
+
+// Resolves one sub-round (each thread writes only its own vcmap entry: the
+// CAS winner pair of p2 and the reset of p3, :320-332) and marks the
+// receivers of the next sub-round when next_r >= 0.
+__global__ void k_resolve(const u32 *list, u32 cnt, const u32 *hn, u32 *vcmap, const unsigned long long *claim,
+                          u32 tag, int next_r) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const u32 u = list[i];
+        u32 s = vcmap[u];
+        const u32 v = hn[u];
+        if (s == SENTINEL - 1) {
+            const unsigned long long c = claim[u];
+            if ((u32) (c >> 32) == tag) {
+                const u32 p = (u32) c;
+                s = u < p ? u : p;
+            } else {
+                s = SENTINEL;
+            }
+        } else if (s == SENTINEL && v != SENTINEL) {
+            const unsigned long long c = claim[v];
+            if ((u32) (c >> 32) == tag && (u32) c == u) s = u < v ? u : v;
+        }
+        if (next_r >= 0 && s == SENTINEL && v != SENTINEL && !commit_cond(u, v, (u32) next_r)) s = SENTINEL - 1;
+        vcmap[u] = s;
+    }
+}
+
+// Re-pick for list vertices whose target got matched (:336-374).
+__global__ void k_repick(DGraph g, const u32 *list, u32 cnt, const u32 *vcmap, u32 *hn, u32 seed, u32 *heavy,
+                         u32 *heavy_cnt) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < cnt; base += stride) {
+        const u64 i = base + threadIdx.x;
+        bool is_heavy = false;
+        u32 u = 0;
+        if (i < cnt) {
+            u = list[i];
+            const u32 h = hn[u];
+            if (vcmap[u] == SENTINEL && h != SENTINEL && vcmap[h] != SENTINEL) {
+                if (g.rowlen[u] <= THREAD_DEG_MAX) hn[u] = pick_thread<false>(g, vcmap, u, seed);
+                else is_heavy = true;
+            }
+        }
+        u32 slot = warp_append(heavy_cnt, is_heavy);
+        if (is_heavy) heavy[slot] = u;
+    }
+}
+
+__global__ void k_count_unmapped(const u32 *vcmap, u32 n, u32 *out) {
+    u32 c = 0;
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) c += vcmap[u] == SENTINEL;
+    c = warp_sum<u32>(c);
+    if (lane_id() == 0 && c) atomicAdd(out, c);
+}
+
+// Twin digest: sum over neighbours of (h + h^2), h = pod_hash(v) in u64
+// (:454-466). One warp per candidate.
+__global__ void k_twin_digest(DGraph g, const u32 *cands, const u32 *cnt, unsigned long long *dig) {
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    const u32 c = *cnt;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < c; i += warps) {
+        const u32 u = cands[i];
+        const u64 beg = g.rowptr[u];
+        const u32 len = g.rowlen[u];
+        unsigned long long s = 0;
+        for (u32 t = lane_id(); t < len; t += 32) {
+            unsigned long long y = murmur3_u32(g.adj[beg + t]);
+            s += y * y + y;
+        }
+        s = warp_sum<unsigned long long>(s);
+        if (lane_id() == 0) dig[i] = s;
+    }
+}
+
+// Relative digest: neighbour of minimum degree, then maximum edge weight,
+// then lowest id (:545-565 with the id tie rule). One warp per candidate.
+__global__ void k_rel_digest(DGraph g, const u32 *cands, const u32 *cnt, u32 *dig) {
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    const u32 c = *cnt;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < c; i += warps) {
+        const u32 u = cands[i];
+        const u64 beg = g.rowptr[u];
+        const u32 len = g.rowlen[u];
+        unsigned long long best = ~0ull;
+        u32 bv = SENTINEL;
+        for (u32 t = lane_id(); t < len; t += 32) {
+            const u32 v = g.adj[beg + t];
+            const u32 d = g.rowlen[v];
+            const s32 w = g_ew(g, beg + t);
+            const unsigned long long key = ((unsigned long long) d << 32) | (u32) (INT32_MAX - w);
+            if (key < best || (key == best && v < bv)) {
+                best = key;
+                bv = v;
+            }
+        }
+        unsigned long long kmin = best;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long y = __shfl_xor_sync(FULL, kmin, o);
+            kmin = y < kmin ? y : kmin;
+        }
+        const u32 vmin = __reduce_min_sync(FULL, best == kmin ? bv : SENTINEL);
+        if (lane_id() == 0) dig[i] = vmin;
+    }
+}
+
+// Pairs sorted candidates: ranks 2j and 2j+1 within a digest group match.
+__global__ void k_pair(const u32 *cands, const u32 *gid, const u32 *gstart, u32 cnt, u32 *vcmap) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const u32 rank = i - gstart[gid[i]];
+        if (rank & 1u) {
+            const u32 a = cands[i - 1], b = cands[i];
+            const u32 cv = a < b ? a : b;
+            vcmap[a] = cv;
+            vcmap[b] = cv;
+        }
+    }
+}
+
+__global__ void k_singletons(u32 *vcmap, u32 n) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+        if (vcmap[u] == SENTINEL) vcmap[u] = u;
+}
+
+__global__ void k_final_map(const u32 *vcmap, const u32 *rank, u32 *mapping, u32 n) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+        mapping[u] = rank[vcmap[u]];
+}
+
+// matchHash (:205-253) under the grouping rule: stable sort by digest, then
+// pair neighbours in each group.
+template<typename K>
+void pair_by_digest(Ctx &ctx, u32 *cands, K *keys, u32 cnt, u32 *vcmap) {
+    if (cnt < 2) return;
+    ScratchScope ss(ctx.arena);
+    radix_sort_pairs<K>(ctx, keys, cands, cnt, 0, 8 * (int) sizeof(K));
+    u32 *gid = ctx.balloc<u32>(cnt);
+    u32 *gstart = ctx.balloc<u32>(cnt);
+    device_scan<u32>(
+        ctx, cnt, [=] __device__(u64 i) -> u32 { return (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u; },
+        [=] __device__(u64 i, u32 p, u32 v) {
+            gid[i] = p + v - 1;
+            if (v) gstart[p] = (u32) i;
+        },
+        (u32 *) nullptr);
+    k_pair<<<ctx.grid(cnt, BLOCK), BLOCK, 0, ctx.stream>>>(cands, gid, gstart, cnt, vcmap);
+    HP_LAUNCH_CHECK();
+}
+
+u32 count_unmapped(Ctx &ctx, const u32 *vcmap, u32 n) {
+    ctx.zero_counters();
+    k_count_unmapped<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, n, &ctx.d_status->cnt[1]);
+    HP_LAUNCH_CHECK();
+    return ctx.read_status().cnt[1];
+}
+
+} // namespace
+
+u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
+    const u32 n = g.n;
+    if (n == 0) return 0;
+    ScratchScope ss(ctx.arena);
+    u32 *vcmap = ctx.balloc<u32>(n);
+    u32 *hn = ctx.balloc<u32>(n);
+    u32 *list = ctx.balloc<u32>(n);
+    u32 *list2 = ctx.balloc<u32>(n);
+    u32 *heavy = ctx.balloc<u32>(n);
+    unsigned long long *claim = ctx.balloc<unsigned long long>(n);
+    HP_CUDA(cudaMemsetAsync(claim, 0xFF, sizeof(unsigned long long) * n, ctx.stream));
+    u32 *heavy_cnt = &ctx.d_status->cnt[2];
+    const u32 seed = MATCH_SEED;
+    const u32 wgrid = ctx.grid((u64) n * 32, BLOCK);
+
+    ctx.zero_counters();
+    k_match_init<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(g, vcmap, hn, seed, heavy, heavy_cnt);
+    k_pick_heavy<true><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, seed, heavy, heavy_cnt);
+    device_iota(ctx, list, n);
+    HP_LAUNCH_CHECK();
+
+    u32 cnt = n;
+    u32 round = 0, epoch = 0;
+    while (cnt > 0) {
+        const u32 round_seed = seed ^ (round * 0x9e3779b1u);
+        const u32 grid = ctx.grid(cnt, BLOCK);
+        k_mark<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, 0);
+        for (u32 r = 0; r < 4; ++r) {
+            ++epoch;
+            const u32 tag = 0xFFFFFFFFu - epoch;
+            k_claim<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag);
+            k_resolve<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag, r < 3 ? (int) r + 1 : -1);
+        }
+        ctx.zero_counters();
+        k_repick<<<grid, BLOCK, 0, ctx.stream>>>(g, list, cnt, vcmap, hn, round_seed, heavy, heavy_cnt);
+        k_pick_heavy<false><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, heavy, heavy_cnt);
+        HP_LAUNCH_CHECK();
+        const u32 *l = list;
+        device_select(
+            ctx, cnt, [=] __device__(u64 i) -> bool {
+                const u32 u = l[i];
+                return vcmap[u] == SENTINEL && hn[u] != SENTINEL;
+            },
+            [=] __device__(u64 i) -> u32 { return l[i]; }, list2, &ctx.d_status->cnt[0]);
+        cnt = ctx.read_status().cnt[0];
+        std::swap(list, list2);
+        ++round;
+        if (round > 100000) throw HpError{HP_ERR_DEVICE, "matching did not converge"};
+    }
+
+    u32 unmapped = count_unmapped(ctx, vcmap, n);
+    // leaf matching (:395-425)
+    if ((u64) unmapped * 4 > (u64) n) {
+        ScratchScope s2(ctx.arena);
+        u32 *cands = ctx.balloc<u32>(n);
+        u32 *dig = ctx.balloc<u32>(n);
+        ctx.zero_counters();
+        const DGraph gg = g;
+        device_scan<u32>(
+            ctx, n, [=] __device__(u64 i) -> u32 { return (vcmap[i] == SENTINEL && gg.rowlen[i] == 1) ? 1u : 0u; },
+            [=] __device__(u64 i, u32 p, u32 v) {
+                if (v) {
+                    cands[p] = (u32) i;
+                    dig[p] = gg.adj[gg.rowptr[i]];
+                }
+            },
+            &ctx.d_status->cnt[0]);
+        u32 c = ctx.read_status().cnt[0];
+        pair_by_digest<u32>(ctx, cands, dig, c, vcmap);
+        unmapped = count_unmapped(ctx, vcmap, n);
+    }
+    // twin matching (:427-524)
+    if ((u64) unmapped * 4 > (u64) n) {
+        ScratchScope s2(ctx.arena);
+        u32 *cands = ctx.balloc<u32>(n);
+        unsigned long long *dig = ctx.balloc<unsigned long long>(n);
+        ctx.zero_counters();
+        device_select(
+            ctx, n, [=] __device__(u64 i) -> bool { return vcmap[i] == SENTINEL; },
+            [=] __device__(u64 i) -> u32 { return (u32) i; }, cands, &ctx.d_status->cnt[0]);
+        k_twin_digest<<<wgrid, BLOCK, 0, ctx.stream>>>(g, cands, &ctx.d_status->cnt[0], dig);
+        HP_LAUNCH_CHECK();
+        u32 c = ctx.read_status().cnt[0];
+        pair_by_digest<unsigned long long>(ctx, cands, dig, c, vcmap);
+        unmapped = count_unmapped(ctx, vcmap, n);
+    }
+    // relative matching (:526-571)
+    if ((u64) unmapped * 4 > (u64) n) {
+        ScratchScope s2(ctx.arena);
+        u32 *cands = ctx.balloc<u32>(n);
+        u32 *dig = ctx.balloc<u32>(n);
+        ctx.zero_counters();
+        device_select(
+            ctx, n, [=] __device__(u64 i) -> bool { return vcmap[i] == SENTINEL; },
+            [=] __device__(u64 i) -> u32 { return (u32) i; }, cands, &ctx.d_status->cnt[0]);
+        k_rel_digest<<<wgrid, BLOCK, 0, ctx.stream>>>(g, cands, &ctx.d_status->cnt[0], dig);
+        HP_LAUNCH_CHECK();
+        u32 c = ctx.read_status().cnt[0];
+        pair_by_digest<u32>(ctx, cands, dig, c, vcmap);
+    }
+    // coarse ids (:611-641)
+    k_singletons<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, n);
+    HP_LAUNCH_CHECK();
+    u32 *rank = list2;
+    ctx.zero_counters();
+    device_scan<u32>(
+        ctx, n, [=] __device__(u64 i) -> u32 { return vcmap[i] == (u32) i ? 1u : 0u; },
+        [=] __device__(u64 i, u32 p, u32 v) {
+            if (v) rank[i] = p;
+        },
+        &ctx.d_status->cnt[0]);
+    k_final_map<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, rank, mapping, n);
+    HP_LAUNCH_CHECK();
+    return ctx.read_status().cnt[0];
+}
+
+} // namespace hp

@@ -1,0 +1,268 @@
+#include "solver.cuh"
+#include "prims.cuh"
+
+#include <chrono>
+#include <cmath>
+
+#include "../host/initial_partition.h"
+
+namespace hp {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double ms_since(Clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
+}
+
+__global__ void k_project(const u32 *coarse_part, const u32 *map, u32 *fine_part, u32 n) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+        fine_part[u] = coarse_part[map[u]];
+}
+
+__global__ void k_scatter_leaf(const u32 *tmp, const u32 *n_to_o, u32 n, u32 offset, u32 *global_part) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x)
+        global_part[n_to_o[u]] = offset + tmp[u];
+}
+
+__global__ void k_compose(const u32 *outer, const u32 *inner, u32 n, u32 *out) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) out[u] = outer[inner[u]];
+}
+
+// Downloads the coarsest graph with rows in canonical (sorted) order.
+HostCSR download_sorted(Ctx &ctx, const DGraph &g) {
+    HostCSR h;
+    h.n = g.n;
+    h.m = (u32) g.m;
+    h.xadj.resize((size_t) g.n + 1);
+    h.adj.resize(g.m);
+    h.ew.resize(g.m);
+    h.vw.resize(g.n);
+    graph_download(ctx, g, h.xadj.data(), h.adj.data(), h.ew.data(), h.vw.data());
+    sort_rows(h);
+    return h;
+}
+
+struct Hierarchy {
+    std::vector<DGraph> graphs;
+    std::vector<u32 *> maps;
+};
+
+// Coarsen while n > 8k (solver.h:343-347); stops early if a level makes no
+// progress.
+void coarsen(Ctx &ctx, const DGraph &g, u32 k, Hierarchy &H, SolveStats *stats) {
+    H.graphs.push_back(g);
+    while (H.graphs.back().n > 8 * k) {
+        const DGraph cur = H.graphs.back();
+        auto t0 = Clock::now();
+        u32 *mp = ctx.falloc<u32>(cur.n);
+        const u32 nc = match_graph(ctx, cur, mp);
+        if (stats) stats->coarsening_ms += ms_since(t0);
+        if (nc == cur.n) break;
+        auto t1 = Clock::now();
+        DGraph c = contract_graph(ctx, cur, mp, nc);
+        if (stats) stats->contraction_ms += ms_since(t1);
+        H.graphs.push_back(c);
+        H.maps.push_back(mp);
+    }
+    if (stats) {
+        stats->levels = (u32) H.graphs.size();
+        for (const DGraph &x: H.graphs) {
+            stats->level_n.push_back(x.n);
+            stats->level_m.push_back(x.m);
+        }
+    }
+}
+
+// Uncoarsen + refine every level (solver.h:381-398).
+void uncoarsen(Ctx &ctx, Hierarchy &H, u32 *coarse_part, u32 *part_out, u32 k, s32 lmax, bool ultra, s64 &obj,
+               s32 &maxw, const DistOracle *D, SolveStats *stats) {
+    u32 *cpart = coarse_part;
+    for (size_t l = H.maps.size(); l > 0; --l) {
+        const DGraph &fine = H.graphs[l - 1];
+        auto t0 = Clock::now();
+        u32 *fpart = (l == 1) ? part_out : ctx.falloc<u32>(fine.n);
+        k_project<<<ctx.grid(fine.n, BLOCK), BLOCK, 0, ctx.stream>>>(cpart, H.maps[l - 1], fpart, fine.n);
+        HP_LAUNCH_CHECK();
+        if (stats) {
+            ctx.sync();
+            stats->uncontraction_ms += ms_since(t0);
+        }
+        auto t1 = Clock::now();
+        jet_refine(ctx, fine, fpart, k, lmax, ultra, (u32) (l - 1), obj, maxw, D);
+        if (stats) stats->refinement_ms += ms_since(t1);
+        cpart = fpart;
+    }
+    if (H.maps.empty())
+        HP_CUDA(cudaMemcpyAsync(part_out, cpart, sizeof(u32) * H.graphs[0].n, cudaMemcpyDeviceToDevice, ctx.stream));
+}
+
+} // namespace
+
+s32 lmax_of(s64 total_weight, u32 k, double eps) {
+    return (s32) std::ceil((1.0 + eps) * ((double) total_weight / (double) k));
+}
+
+size_t arena_estimate(u32 n, u64 m, bool has_ew, bool has_vw) {
+    // input graph + hierarchy (about 3x the input rows at worst for the padded
+    // levels) + Jet state (~12 n words) + matching / contraction scratch.
+    const double in = 4.0 * ((double) n + 1) * 2 + 4.0 * (double) m * (has_ew ? 2 : 1) + (has_vw ? 4.0 * n : 0.0);
+    const double hier = 3.0 * (8.0 * (double) m + 16.0 * (double) n);
+    const double scratch = 4.0 * (14.0 * (double) n) + 16.0 * (double) m;
+    const double total = in + hier + scratch + (64ull << 20);
+    return (size_t) (total * 1.15);
+}
+
+s64 solve_partition(Ctx &ctx, const DGraph &g, u32 k, double eps, bool ultra, u64 seed, u32 *part,
+                    SolveStats *stats) {
+    if (k == 0) throw HpError{HP_ERR_ARG, "k must be positive"};
+    if (k > MAX_K) throw HpError{HP_ERR_ARG, "k too large"};
+    if (g.n == 0) return 0;
+    if (k == 1) {
+        HP_CUDA(cudaMemsetAsync(part, 0, sizeof(u32) * g.n, ctx.stream));
+        ctx.sync();
+        return 0;
+    }
+    const size_t front_mark = ctx.arena.front_mark();
+    const s32 lmax = lmax_of(g.total_vw, k, eps);
+    Hierarchy H;
+    coarsen(ctx, g, k, H, stats);
+    const DGraph &coarsest = H.graphs.back();
+    // initial partitioning on the host (kway_core.h:1573-1588)
+    auto t0 = Clock::now();
+    HostCSR hc = download_sorted(ctx, coarsest);
+    std::vector<u32> hpart;
+    initial_kway(hc, k, eps, seed, hpart);
+    u32 *cpart = ctx.falloc<u32>(coarsest.n);
+    HP_CUDA(cudaMemcpyAsync(cpart, hpart.data(), sizeof(u32) * coarsest.n, cudaMemcpyHostToDevice, ctx.stream));
+    s64 obj = edge_cut_dev(ctx, coarsest, cpart);
+    s32 *bw = ctx.falloc<s32>(k);
+    block_weights(ctx, coarsest, cpart, k, bw);
+    s32 maxw = max_block_weight(ctx, bw, k);
+    if (stats) {
+        stats->initial_ms += ms_since(t0);
+        stats->initial_obj = obj;
+        stats->initial_maxw = maxw;
+        stats->lmax = lmax;
+    }
+    uncoarsen(ctx, H, cpart, part, k, lmax, ultra, obj, maxw, nullptr, stats);
+    ctx.sync();
+    ctx.arena.front_release(front_mark);
+    if (stats) {
+        stats->final_obj = obj;
+        stats->final_maxw = maxw;
+    }
+    return obj;
+}
+
+namespace {
+
+// recursive_multisection_device (hierarchical_multisection.h:56-235)
+void hm_recurse(Ctx &ctx, const DGraph &g, const u32 *n_to_o, const std::vector<u32> &hier, u32 level,
+                std::vector<u32> &identifier, const std::vector<u32> &index_vec, const std::vector<u32> &k_rem,
+                double eps, s64 global_w, u32 global_k, u64 seed, bool ultra, u32 *global_part, SolveStats *stats) {
+    const u32 l = (u32) hier.size();
+    const u32 k_here = hier[level];
+    const u64 depth = identifier.size();
+    const double imb = adaptive_imbalance(eps, global_w, global_k, g.total_vw, k_rem[l - 1 - depth], l - depth);
+    const size_t mark = ctx.arena.front_mark();
+    u32 *tmp = ctx.falloc<u32>(g.n);
+    SolveStats sub;
+    solve_partition(ctx, g, k_here, imb, ultra, seed, tmp, stats ? &sub : nullptr);
+    if (stats) stats->add(sub);
+    if (depth == l - 1) {
+        u32 offset = 0;
+        for (u32 i = 0; i + 1 < l; ++i) offset += identifier[i] * index_vec[index_vec.size() - 1 - i];
+        k_scatter_leaf<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(tmp, n_to_o, g.n, offset, global_part);
+        HP_LAUNCH_CHECK();
+        ctx.sync();
+        ctx.arena.front_release(mark);
+        return;
+    }
+    for (u32 id = 0; id < k_here; ++id) {
+        const size_t m2 = ctx.arena.front_mark();
+        u32 *sub_n_to_o_local = ctx.falloc<u32>(g.n);
+        u32 sub_n = 0;
+        DGraph sg = graph_induced(ctx, g, tmp, id, sub_n_to_o_local, sub_n);
+        if (sub_n == 0) {
+            ctx.arena.front_release(m2);
+            continue;
+        }
+        u32 *sub_n_to_o = ctx.falloc<u32>(sub_n);
+        k_compose<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(n_to_o, sub_n_to_o_local, sub_n, sub_n_to_o);
+        HP_LAUNCH_CHECK();
+        identifier.push_back(id);
+        hm_recurse(ctx, sg, sub_n_to_o, hier, level - 1, identifier, index_vec, k_rem, eps, global_w, global_k, seed,
+                   ultra, global_part, stats);
+        identifier.pop_back();
+        ctx.arena.front_release(m2);
+    }
+    ctx.arena.front_release(mark);
+}
+
+} // namespace
+
+s64 solve_mapping(Ctx &ctx, const DGraph &g, const std::vector<u32> &hier, const std::vector<s32> &dist, double eps,
+                  int mode, u64 seed, u32 *part, SolveStats *stats) {
+    const size_t front_mark = ctx.arena.front_mark();
+    DistOracle D = make_dist_oracle(ctx, hier, dist);
+    const u32 k = D.k;
+    const u32 l = (u32) hier.size();
+    s64 J = 0;
+    if (g.n == 0) return 0;
+    if (mode == 0) {
+        // ProMapSolver::internal_solve (promap_solver.h:244-299)
+        const s32 lmax = lmax_of(g.total_vw, k, eps);
+        Hierarchy H;
+        coarsen(ctx, g, k, H, stats);
+        const DGraph &coarsest = H.graphs.back();
+        auto t0 = Clock::now();
+        HostCSR hc = download_sorted(ctx, coarsest);
+        std::vector<u32> hpart;
+        global_multisection(hc, hier, eps, seed, hpart);
+        u32 *cpart = ctx.falloc<u32>(coarsest.n);
+        HP_CUDA(cudaMemcpyAsync(cpart, hpart.data(), sizeof(u32) * coarsest.n, cudaMemcpyHostToDevice, ctx.stream));
+        J = comm_cost_dev(ctx, coarsest, cpart, D);
+        s32 *bw = ctx.falloc<s32>(k);
+        block_weights(ctx, coarsest, cpart, k, bw);
+        s32 maxw = max_block_weight(ctx, bw, k);
+        if (stats) {
+            stats->initial_ms += ms_since(t0);
+            stats->initial_obj = J;
+            stats->initial_maxw = maxw;
+            stats->lmax = lmax;
+        }
+        uncoarsen(ctx, H, cpart, part, k, lmax, false, J, maxw, &D, stats);
+        if (stats) {
+            stats->final_obj = J;
+            stats->final_maxw = maxw;
+        }
+    } else {
+        // hierarchical_multisection (hierarchical_multisection.h:237-307)
+        std::vector<u32> index_vec = {1};
+        for (u32 i = 0; i + 1 < l; ++i) index_vec.push_back(index_vec[i] * hier[i]);
+        std::vector<u32> k_rem(l);
+        u32 p = 1;
+        for (u32 i = 0; i < l; ++i) {
+            k_rem[i] = p * hier[i];
+            p *= hier[i];
+        }
+        u32 *n_to_o = ctx.falloc<u32>(g.n);
+        device_iota(ctx, n_to_o, g.n);
+        std::vector<u32> identifier;
+        hm_recurse(ctx, g, n_to_o, hier, l - 1, identifier, index_vec, k_rem, eps, g.total_vw, k, seed, mode == 2,
+                   part, stats);
+        J = comm_cost_dev(ctx, g, part, D);
+        if (stats) {
+            s32 *bw = ctx.falloc<s32>(k);
+            block_weights(ctx, g, part, k, bw);
+            stats->final_obj = J;
+            stats->final_maxw = max_block_weight(ctx, bw, k);
+            stats->lmax = lmax_of(g.total_vw, k, eps);
+        }
+    }
+    ctx.sync();
+    ctx.arena.front_release(front_mark);
+    return J;
+}
+
+} // namespace hp

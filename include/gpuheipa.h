@@ -1,0 +1,164 @@
+/*
+ * C ABI of the B200 multilevel graph partitioner / process mapper.
+ *
+ * Every entry point returns an int status (HP_OK == 0) and never exits or
+ * aborts; hp_last_error() returns the message of the last failure on a
+ * context. Host buffers are owned by the caller. Device memory is owned by the
+ * context's arena, which allocates LIFO like the reference's
+ * KokkosMemoryStack (src/datastructures/kokkos_memory_stack.h:36-206): graph
+ * handles must be freed in reverse order of creation.
+ *
+ * The reference exposes this path only as header-only C++ templates; the
+ * comment above each function names the reference interface it replaces.
+ * Conventions: n = vertices, m = directed CSR entries (2x undirected edges,
+ * src/datastructures/host_graph.h:195), ids uint32, weights int32 (>= 1),
+ * objectives int64. A NULL weight array means unit weights ("uniform").
+ */
+#ifndef GPUHEIPA_H
+#define GPUHEIPA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    HP_OK = 0,
+    HP_ERR_ARG = 1,
+    HP_ERR_CUDA = 2,
+    HP_ERR_OOM = 3,
+    HP_ERR_IO = 4,
+    HP_ERR_GRAPH = 5,
+    HP_ERR_DEVICE = 6
+};
+
+/* Mapping modes for hp_map / hp_map_graph (GPU-HeiProMap --config). */
+enum { HP_MAP_IM = 0, HP_MAP_HM = 1, HP_MAP_HM_ULTRA = 2 };
+
+typedef struct hp_ctx hp_ctx;
+typedef struct hp_graph hp_graph;
+typedef struct hp_jet hp_jet;
+typedef struct hp_host_graph hp_host_graph;
+
+/* ---- context ------------------------------------------------------------------ */
+
+/* Replaces Kokkos::initialize + initialize_kokkos_memory_stack
+ * (app/GPU-HeiPa.cpp:44, src/datastructures/kokkos_memory_stack.h:57). */
+int hp_ctx_create(int device, size_t arena_bytes, hp_ctx **out);
+/* Replaces destroy(mem_stack) + Kokkos::finalize (kokkos_memory_stack.h:195-206). */
+int hp_ctx_destroy(hp_ctx *ctx);
+/* Message of the last failed call on ctx ("" if none). */
+const char *hp_last_error(const hp_ctx *ctx);
+/* Arena bytes a solve of an (n, m) graph needs; replaces the sizing rules of
+ * configuration.h:79 and promap_solver.h:307-311. */
+size_t hp_arena_estimate(uint32_t n, uint64_t m, int has_edge_weights, int has_vertex_weights);
+/* Peak arena bytes used so far. */
+size_t hp_arena_peak(const hp_ctx *ctx);
+
+/* ---- device graphs -------------------------------------------------------- */
+
+/* Replaces from_HostGraph (src/datastructures/graph.h:63-125). Validates ids,
+ * self loops and weights on the device. */
+int hp_graph_upload(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                    const int32_t *ew, const int32_t *vw, hp_graph **out);
+/* Replaces free_graph (graph.h:438-443); LIFO order. */
+int hp_graph_free(hp_ctx *ctx, hp_graph *g);
+/* n, m (directed entries present) and total vertex weight of a device graph. */
+int hp_graph_info(const hp_graph *g, uint32_t *n, uint64_t *m, int64_t *total_vw);
+/* Replaces to_host_graph (graph.h:413-436): compact CSR copy to host arrays
+ * (xadj n+1, adj m, ew m, vw n; any may be NULL). Row order is the device's. */
+int hp_graph_download(hp_ctx *ctx, const hp_graph *g, uint32_t *xadj, uint32_t *adj, int32_t *ew, int32_t *vw);
+
+/* ---- phase kernels -------------------------------------------------------- */
+
+/* Replaces two_hop_matcher_get_mapping (src/coarsening/two_hop_matching.h:573)
+ * with deterministic tie rules; writes mapping (n entries, host). */
+int hp_match(hp_ctx *ctx, const hp_graph *g, uint32_t *mapping, uint32_t *n_coarse);
+/* Replaces from_Graph_Mapping (src/datastructures/graph.h:127-390): contracts
+ * g with a host mapping (values < n_coarse) into a new device graph. */
+int hp_contract(hp_ctx *ctx, const hp_graph *g, const uint32_t *mapping, uint32_t n_coarse, hp_graph **out);
+/* Replaces jet_refine (src/refinement/jet_label_propagation.h:926) when
+ * hier == NULL, and ProMap_jet_refine (promap_jet_label_propagation.h:1218)
+ * otherwise; part (host, n) is refined in place; obj and maxw are the running
+ * objective and maximum block weight (in/out). */
+int hp_jet_refine(hp_ctx *ctx, const hp_graph *g, uint32_t k, int32_t lmax, int ultra, uint32_t level,
+                  uint32_t *part, int64_t *obj, int32_t *maxw, const uint32_t *hier, const int32_t *dist,
+                  uint32_t levels);
+
+/* One Jet iteration at a time, for stepping and inspection (the phases of
+ * jet_refine: jet_lp :182, rebalance_weak :592, rebalance_strong :356,
+ * perform_moves :753; ProMap variants likewise). */
+int hp_jet_begin(hp_ctx *ctx, const hp_graph *g, uint32_t k, int32_t lmax, const uint32_t *part,
+                 const uint32_t *hier, const int32_t *dist, uint32_t levels, hp_jet **out);
+int hp_jet_lp(hp_jet *jet, uint32_t ratio_pct, uint32_t *moves, uint32_t *count);
+int hp_jet_weak(hp_jet *jet, uint32_t *moves, uint32_t *count);
+int hp_jet_strong(hp_jet *jet, uint32_t *moves, uint32_t *count);
+/* Applies the moves selected by the last lp/weak/strong call. */
+int hp_jet_perform(hp_jet *jet, int64_t *obj, int32_t *maxw);
+/* Copies the per-vertex Jet state (any pointer may be NULL). */
+int hp_jet_state(hp_jet *jet, uint32_t *map, int32_t *bw, uint32_t *dest_part, int32_t *gain1, uint32_t *lock,
+                 uint32_t *dest_cache, int32_t *gain_cache);
+int hp_jet_end(hp_jet *jet);
+
+/* Replaces edge_cut (src/utility/edge_cut.h:71-90) and comm_cost
+ * (src/utility/comm_cost.h:36-56) with int64 sums. part is a host array. */
+int hp_edge_cut(hp_ctx *ctx, const hp_graph *g, const uint32_t *part, int64_t *cut);
+int hp_comm_cost(hp_ctx *ctx, const hp_graph *g, const uint32_t *part, const uint32_t *hier, const int32_t *dist,
+                 uint32_t levels, int64_t *J);
+
+/* ---- whole solves ---------------------------------------------------------- */
+
+/* Replaces Solver(config).solve(HostGraph&) (src/datastructures/solver.h:248)
+ * for GPU-HeiPa --config default|ultra. Host CSR in, host partition out. */
+int hp_partition(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj, const int32_t *ew,
+                 const int32_t *vw, uint32_t k, double imbalance, int ultra, uint64_t seed, uint32_t *part,
+                 int64_t *cut);
+/* Same on an uploaded graph (the device-resident path). */
+int hp_partition_graph(hp_ctx *ctx, const hp_graph *g, uint32_t k, double imbalance, int ultra, uint64_t seed,
+                       uint32_t *part, int64_t *cut);
+/* Replaces ProMapSolver<DistanceOracleMatrix>(config).solve / solve_multisection
+ * (src/datastructures/promap_solver.h:146,238) for GPU-HeiProMap --config
+ * IM|HM|HM-ultra. Returns J over directed entries in *J. */
+int hp_map(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj, const int32_t *ew,
+           const int32_t *vw, const uint32_t *hier, const int32_t *dist, uint32_t levels, double imbalance, int mode,
+           uint64_t seed, uint32_t *part, int64_t *J);
+int hp_map_graph(hp_ctx *ctx, const hp_graph *g, const uint32_t *hier, const int32_t *dist, uint32_t levels,
+                 double imbalance, int mode, uint64_t seed, uint32_t *part, int64_t *J);
+
+/* Phase timings (ms) of the last solve on ctx: coarsening, contraction,
+ * initial partitioning, uncontraction, refinement (solver.h:319-328 keys). */
+int hp_last_solve_stats(const hp_ctx *ctx, double *phase_ms5, int64_t *initial_obj, int32_t *lmax,
+                        uint32_t *levels);
+
+/* Enables CUDA-event timing of the contraction and Jet-gain kernels on ctx;
+ * hp_kernel_timing reports launches, total ms and algorithmic bytes. */
+int hp_instrument(hp_ctx *ctx, int enable);
+int hp_kernel_timing(hp_ctx *ctx, const char *name, uint64_t *launches, double *ms, double *bytes);
+
+/* ---- host utilities (no device work) --------------------------------------- */
+
+/* Replaces from_file (src/datastructures/host_graph.h:154-247). */
+int hp_read_metis(const char *path, hp_host_graph **out);
+/* Synthetic generators for the benchmark workloads. */
+int hp_gen_grid(uint32_t w, uint32_t h, int32_t w_lo, int32_t w_hi, uint64_t seed, hp_host_graph **out);
+int hp_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, int32_t w_lo, int32_t w_hi,
+                uint64_t seed, int explicit_vw, hp_host_graph **out);
+int hp_gen_rgg3d(uint32_t n, double mean_degree, int32_t w_lo, int32_t w_hi, uint64_t seed, int explicit_vw,
+                 hp_host_graph **out);
+/* Sizes (has_ew/has_vw: 0 when weights are unit) and contents of a host graph. */
+int hp_host_graph_info(const hp_host_graph *g, uint32_t *n, uint64_t *m, int *has_ew, int *has_vw);
+int hp_host_graph_copy(const hp_host_graph *g, uint32_t *xadj, uint32_t *adj, int32_t *ew, int32_t *vw);
+int hp_host_graph_free(hp_host_graph *g);
+/* Writes a METIS file (fmt 0/1/10/11 from the flags). */
+int hp_write_metis(const char *path, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                   const int32_t *ew, const int32_t *vw);
+/* Replaces write_partition (src/utility/util.h:288-329): one id per line. */
+int hp_write_partition(const char *path, const uint32_t *part, uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPUHEIPA_H */
