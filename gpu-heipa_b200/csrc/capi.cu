@@ -481,6 +481,41 @@ int hp_kernel_timing(hp_ctx *ctx, const char *name, uint64_t *launches, double *
     });
 }
 
+int hp_event_record(hp_ctx *ctx, int slot) {
+    if (!ctx) return HP_ERR_ARG;
+    return guarded(ctx, [&] { HP_CUDA(cudaEventRecord(ctx->c.event(slot), ctx->c.stream)); });
+}
+
+int hp_event_elapsed(hp_ctx *ctx, int slot_a, int slot_b, float *ms) {
+    if (!ctx || !ms) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        cudaEvent_t b = ctx->c.event(slot_b);
+        HP_CUDA(cudaEventSynchronize(b));
+        HP_CUDA(cudaEventElapsedTime(ms, ctx->c.event(slot_a), b));
+    });
+}
+
+uint64_t hp_kernel_launches(void) { return hp::g_kernel_launches.load(); }
+
+int hp_profile(hp_ctx *ctx, int enable) {
+    if (!ctx) return HP_ERR_ARG;
+    ctx->c.prof.enabled = enable != 0;
+    ctx->c.prof.clear();
+    return HP_OK;
+}
+
+int hp_profile_entry(const hp_ctx *ctx, uint32_t index, char *name, size_t name_len, double *ms, uint64_t *count) {
+    if (!ctx || index >= ctx->c.prof.totals.size()) return HP_ERR_ARG;
+    const auto &e = ctx->c.prof.totals[index];
+    if (name && name_len) {
+        std::strncpy(name, e.first.c_str(), name_len - 1);
+        name[name_len - 1] = 0;
+    }
+    if (ms) *ms = e.second;
+    if (count) *count = ctx->c.prof.counts[index].second;
+    return HP_OK;
+}
+
 int hp_read_metis(const char *path, hp_host_graph **out) {
     if (!path || !out) return HP_ERR_ARG;
     *out = nullptr;

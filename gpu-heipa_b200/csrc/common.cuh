@@ -1,5 +1,6 @@
 // Common device-side definitions for the sm_100a partitioner kernels.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -126,7 +127,34 @@ __device__ __forceinline__ u32 warp_append(u32 *counter, bool pred) {
     return base + (u32) __popc(mask & ((1u << lane_id()) - 1u));
 }
 
+// Block-wide version of warp_append: one global atomic per block. All
+// threads of the block must call it; `sm` holds 33 u32.
+__device__ __forceinline__ u32 block_append(u32 *counter, bool pred, u32 *sm) {
+    const unsigned mask = __ballot_sync(FULL, pred);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) sm[w] = (u32) __popc(mask);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        u32 tot = 0;
+        for (u32 i = 0; i < (blockDim.x >> 5); ++i) {
+            const u32 c = sm[i];
+            sm[i] = tot;
+            tot += c;
+        }
+        sm[32] = tot ? atomicAdd(counter, tot) : 0u;
+    }
+    __syncthreads();
+    const u32 r = sm[32] + sm[w] + (u32) __popc(mask & ((1u << lane) - 1u));
+    __syncthreads();
+    return r;
+}
+
 __device__ __forceinline__ void set_error(u32 *err, u32 bits) { atomicOr(err, bits); }
+
+// Number of kernels this process has launched (every launch site calls
+// note_launch()).
+extern std::atomic<unsigned long long> g_kernel_launches;
+inline void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 
 // Grid sizing: a multiple of the SM count, capped by the work.
 inline u32 grid_for(u64 items, u32 per_block, u32 max_blocks = NUM_SMS_HINT * 16) {

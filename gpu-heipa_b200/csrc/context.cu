@@ -1,6 +1,10 @@
 #include "context.h"
 
+#include <chrono>
+
 namespace hp {
+
+std::atomic<unsigned long long> g_kernel_launches{0};
 
 static constexpr size_t ALIGN = 256;
 
@@ -122,8 +126,46 @@ void Instr::destroy() {
     pool.clear();
 }
 
+void PhaseProf::add(const char *name, double ms) {
+    for (size_t i = 0; i < totals.size(); ++i)
+        if (totals[i].first == name) {
+            totals[i].second += ms;
+            counts[i].second += 1;
+            return;
+        }
+    totals.emplace_back(name, ms);
+    counts.emplace_back(name, 1);
+}
+
+static double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+ProfScope::ProfScope(Ctx &ctx, const char *nm) : c(ctx), name(nm) {
+    if (!c.prof.enabled) return;
+    cudaStreamSynchronize(c.stream);
+    t0 = now_ms();
+}
+
+ProfScope::~ProfScope() {
+    if (!c.prof.enabled) return;
+    cudaStreamSynchronize(c.stream);
+    c.prof.add(name, now_ms() - t0);
+}
+
+cudaEvent_t Ctx::event(int slot) {
+    if (slot < 0 || slot >= 8) throw HpError{HP_ERR_ARG, "event slot out of range"};
+    if (!events[slot]) HP_CUDA(cudaEventCreate(&events[slot]));
+    return events[slot];
+}
+
 void Ctx::destroy() {
     if (stream) cudaStreamSynchronize(stream);
+    for (cudaEvent_t &e: events)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
     instr.destroy();
     arena.destroy();
     if (d_status) cudaFree(d_status);

@@ -95,6 +95,20 @@ struct Instr {
     void destroy();
 };
 
+// Diagnostic phase timers: when enabled, a scope synchronises the stream on
+// entry and exit and accumulates wall-clock milliseconds per name. Off by
+// default (no synchronisation is added to the normal path).
+struct PhaseProf {
+    bool enabled = false;
+    std::vector<std::pair<std::string, double> > totals;
+    std::vector<std::pair<std::string, u64> > counts;
+    void add(const char *name, double ms);
+    void clear() {
+        totals.clear();
+        counts.clear();
+    }
+};
+
 struct Ctx {
     int device = 0;
     int sm_count = NUM_SMS_HINT;
@@ -105,6 +119,9 @@ struct Ctx {
     std::string last_error;
     bool owns_arena = true;
     Instr instr;
+    PhaseProf prof;
+    cudaEvent_t events[8] = {};
+    cudaEvent_t event(int slot);  // created on first use
 
     void init(int dev, size_t arena_bytes);
     void destroy();
@@ -127,6 +144,15 @@ struct Ctx {
         u64 cap = (u64) sm_count * 16;
         return (u32) (b > cap ? cap : b);
     }
+};
+
+// RAII scope for PhaseProf.
+struct ProfScope {
+    Ctx &c;
+    const char *name;
+    double t0 = 0;
+    ProfScope(Ctx &ctx, const char *nm);
+    ~ProfScope();
 };
 
 } // namespace hp

@@ -155,6 +155,10 @@ __global__ void __launch_bounds__(C_WARP_BLOCK) k_contract_warp(CArgs a, const u
     unsigned long long msum = 0;
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const u32 c = wl[i];
+        const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
+        u32 bits = 6;
+        while ((1u << bits) < 2 * cap && bits < C_WARP_BITS) ++bits;
+        const u32 tsz = 1u << bits;
         for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
             const u32 u = a.mlist[mi];
             const u64 beg = a.g.rowptr[u];
@@ -162,14 +166,14 @@ __global__ void __launch_bounds__(C_WARP_BLOCK) k_contract_warp(CArgs a, const u
             for (u32 t = lane; t < len; t += 32) {
                 const u32 cv = a.map[a.g.adj[beg + t]];
                 if (cv == c) continue;
-                if (!table_insert(tk, tw, C_WARP_SLOTS - 1, hslot(cv, C_WARP_BITS), cv, g_ew(a.g, beg + t)))
+                if (!table_insert(tk, tw, tsz - 1, hslot(cv, bits), cv, g_ew(a.g, beg + t)))
                     set_error(a.err, DEV_ERR_HASH_FULL);
             }
         }
         __syncwarp();
         const u64 out = a.c.rowptr[c];
         u32 cntu = 0;
-        for (u32 s0 = 0; s0 < C_WARP_SLOTS; s0 += 32) {
+        for (u32 s0 = 0; s0 < tsz; s0 += 32) {
             const u32 s = s0 + lane;
             const u32 key = tk[s];
             const bool has = key != EMPTY;
@@ -190,26 +194,22 @@ __global__ void __launch_bounds__(C_WARP_BLOCK) k_contract_warp(CArgs a, const u
     if (lane == 0 && msum) atomicAdd(a.m_out, msum);
 }
 
-// Emits the non-empty slots of a block-wide table into the coarse row.
-template<int NT>
-__device__ __forceinline__ u32 block_emit(u32 *tk, s32 *tw, u32 slots, u64 out, u32 *adj, s32 *ew, bool reset,
+// Emits the non-empty slots of a block-wide table into the coarse row and
+// resets them (thread t owns slots t, t + NT, ...).
+__device__ __forceinline__ u32 block_emit(u32 *tk, s32 *tw, u32 slots, u64 out, u32 *adj, s32 *ew,
                                           u32 *smem_scan) {
-    const u32 per = slots / NT;
-    const u32 s0 = threadIdx.x * per;
     u32 cnt = 0;
-    for (u32 s = s0; s < s0 + per; ++s) cnt += tk[s] != EMPTY;
+    for (u32 s = threadIdx.x; s < slots; s += blockDim.x) cnt += tk[s] != EMPTY;
     u32 tot;
     u32 p = block_exclusive_scan<u32>(cnt, tot, smem_scan);
-    for (u32 s = s0; s < s0 + per; ++s) {
+    for (u32 s = threadIdx.x; s < slots; s += blockDim.x) {
         const u32 key = tk[s];
         if (key != EMPTY) {
             adj[out + p] = key;
             ew[out + p] = tw[s];
             ++p;
-            if (reset) {
-                tk[s] = EMPTY;
-                tw[s] = 0;
-            }
+            tk[s] = EMPTY;
+            tw[s] = 0;
         }
     }
     return tot;
@@ -229,6 +229,11 @@ __global__ void __launch_bounds__(BLOCK) k_contract_block(CArgs a, const u32 *bl
     unsigned long long msum = 0;
     for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
         const u32 c = bl[i];
+        // table of the next power of two >= 2 * capacity (<= C_BLOCK_SLOTS)
+        const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
+        u32 bits = 9;
+        while ((1u << bits) < 2 * cap && bits < C_BLOCK_BITS) ++bits;
+        const u32 tsz = 1u << bits;
         for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
             const u32 u = a.mlist[mi];
             const u64 beg = a.g.rowptr[u];
@@ -236,12 +241,12 @@ __global__ void __launch_bounds__(BLOCK) k_contract_block(CArgs a, const u32 *bl
             for (u32 t = threadIdx.x; t < len; t += blockDim.x) {
                 const u32 cv = a.map[a.g.adj[beg + t]];
                 if (cv == c) continue;
-                if (!table_insert(tk, tw, C_BLOCK_SLOTS - 1, hslot(cv, C_BLOCK_BITS), cv, g_ew(a.g, beg + t)))
+                if (!table_insert(tk, tw, tsz - 1, hslot(cv, bits), cv, g_ew(a.g, beg + t)))
                     set_error(a.err, DEV_ERR_HASH_FULL);
             }
         }
         __syncthreads();
-        const u32 cntu = block_emit<BLOCK>(tk, tw, C_BLOCK_SLOTS, a.c.rowptr[c], a.c.adj, a.c.ew, true, scan_sm);
+        const u32 cntu = block_emit(tk, tw, tsz, a.c.rowptr[c], a.c.adj, a.c.ew, scan_sm);
         if (threadIdx.x == 0) a.c.rowlen[c] = cntu;
         msum += cntu;
         __syncthreads();
@@ -316,6 +321,7 @@ __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u
 } // namespace
 
 DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
+    ProfScope prof(ctx, "contract");
     DGraph c;
     c.n = n_c;
     c.cap = g.m;
@@ -339,7 +345,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     HP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(u32) * n_c, ctx.stream));
     HP_CUDA(cudaMemsetAsync(capsum, 0, sizeof(u32) * n_c, ctx.stream));
     HP_CUDA(cudaMemsetAsync(c.vw, 0, sizeof(s32) * n_c, ctx.stream));
-    k_cluster_stats<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, mapping, cnt, capsum, c.vw);
+    k_cluster_stats<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, mapping, cnt, capsum, c.vw); note_launch();
     HP_LAUNCH_CHECK();
     u32 *rowptr = c.rowptr;
     device_scan<u32>(
@@ -352,7 +358,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     device_scan<u32>(
         ctx, (u64) n_c + 1, [=] __device__(u64 i) -> u32 { return i < n_c ? capsum[i] : 0u; },
         [=] __device__(u64 i, u32 p, u32) { rowptr[i] = p; }, (u32 *) nullptr);
-    k_fill_members<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(mapping, g.n, cursor, mlist);
+    k_fill_members<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(mapping, g.n, cursor, mlist); note_launch();
     HP_LAUNCH_CHECK();
 
     ctx.zero_counters();
@@ -361,7 +367,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     const size_t rec0 = ctx.instr.pending.size();
     ctx.instr.begin(ctx.stream, "contract", 0.0);
     k_contract_small<<<ctx.grid(n_c, BLOCK), BLOCK, 0, ctx.stream>>>(
-        a, wl, &st->cnt[0], bl, &st->cnt[1], hl, &st->cnt[2], hoff, (unsigned long long *) &st->sum[0]);
+        a, wl, &st->cnt[0], bl, &st->cnt[1], hl, &st->cnt[2], hoff, (unsigned long long *) &st->sum[0]); note_launch();
     HP_LAUNCH_CHECK();
     ctx.instr.end(ctx.stream);
     const DevStatus &s1 = ctx.read_status();
@@ -369,7 +375,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     const u64 hslots = (u64) s1.sum[0];
     if (nw) {
         ctx.instr.begin(ctx.stream, "contract", 0.0);
-        k_contract_warp<<<ctx.grid((u64) nw * 32, C_WARP_BLOCK), C_WARP_BLOCK, 0, ctx.stream>>>(a, wl, &st->cnt[0]);
+        k_contract_warp<<<ctx.grid((u64) nw * 32, C_WARP_BLOCK), C_WARP_BLOCK, 0, ctx.stream>>>(a, wl, &st->cnt[0]); note_launch();
         HP_LAUNCH_CHECK();
         ctx.instr.end(ctx.stream);
     }
@@ -378,7 +384,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
         HP_CUDA(cudaFuncSetAttribute(k_contract_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         ctx.instr.begin(ctx.stream, "contract", 0.0);
         k_contract_block<<<(u32) std::min<u64>(nb, (u64) ctx.sm_count * 3), BLOCK, smem, ctx.stream>>>(a, bl,
-                                                                                                     &st->cnt[1]);
+                                                                                                     &st->cnt[1]); note_launch();
         HP_LAUNCH_CHECK();
         ctx.instr.end(ctx.stream);
     }
@@ -387,7 +393,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
         s32 *twts = ctx.balloc<s32>(hslots);
         ctx.instr.begin(ctx.stream, "contract", 0.0);
         k_contract_huge<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
-            a, hl, &st->cnt[2], hoff, tkeys, twts);
+            a, hl, &st->cnt[2], hoff, tkeys, twts); note_launch();
         HP_LAUNCH_CHECK();
         ctx.instr.end(ctx.stream);
     }

@@ -9,7 +9,7 @@ __global__ void k_iota(u32 *p, u64 n) {
 
 void device_iota(Ctx &ctx, u32 *p, u64 n) {
     if (n == 0) return;
-    k_iota<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(p, n);
+    k_iota<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(p, n); note_launch();
     HP_LAUNCH_CHECK();
 }
 
@@ -47,10 +47,10 @@ __global__ void k_validate_edges(DGraph g, u32 *err) {
 
 static void finish_graph(Ctx &ctx, DGraph &g, bool validate) {
     ctx.zero_status();
-    k_rows<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, &ctx.d_status->err, &ctx.d_status->sum[0]);
+    k_rows<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, &ctx.d_status->err, &ctx.d_status->sum[0]); note_launch();
     HP_LAUNCH_CHECK();
     if (validate && g.cap > 0) {
-        k_validate_edges<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, &ctx.d_status->err);
+        k_validate_edges<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, &ctx.d_status->err); note_launch();
         HP_LAUNCH_CHECK();
     }
     const DevStatus &s = ctx.read_status();
@@ -122,7 +122,7 @@ void graph_download(Ctx &ctx, const DGraph &g, u32 *xadj, u32 *adj, s32 *ew, s32
         [=] __device__(u64 i, u32 p, u32) { off[i] = p; }, (u32 *) nullptr);
     u32 *dadj = ctx.balloc<u32>(g.m);
     s32 *dew = ctx.balloc<s32>(g.m);
-    k_compact_rows<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, off, dadj, dew);
+    k_compact_rows<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, off, dadj, dew); note_launch();
     HP_LAUNCH_CHECK();
     if (xadj) HP_CUDA(cudaMemcpyAsync(xadj, off, sizeof(u32) * ((u64) g.n + 1), cudaMemcpyDeviceToHost, ctx.stream));
     if (adj && g.m) HP_CUDA(cudaMemcpyAsync(adj, dadj, sizeof(u32) * g.m, cudaMemcpyDeviceToHost, ctx.stream));
@@ -209,7 +209,7 @@ DGraph graph_induced(Ctx &ctx, const DGraph &g, const u32 *part, u32 id, u32 *n_
             }
         },
         counts + 0);
-    k_sub_degrees<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, id, deg);
+    k_sub_degrees<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, id, deg); note_launch();
     HP_LAUNCH_CHECK();
     device_scan<u32>(
         ctx, g.n, [=] __device__(u64 i) -> u32 { return deg[i]; }, [=] __device__(u64 i, u32 p, u32) { eoff[i] = p; },
@@ -227,8 +227,8 @@ DGraph graph_induced(Ctx &ctx, const DGraph &g, const u32 *part, u32 id, u32 *n_
     s.ew = ctx.falloc<s32>(sub_m);
     s.vw = ctx.falloc<s32>(sub_n);
     if (sub_n == 0) return s;
-    k_sub_fill<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, id, local, eoff, s);
-    k_sub_rowlen<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(s, sub_m);
+    k_sub_fill<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, id, local, eoff, s); note_launch();
+    k_sub_rowlen<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(s, sub_m); note_launch();
     HP_LAUNCH_CHECK();
     // total vertex weight of the subgraph
     ctx.zero_counters();

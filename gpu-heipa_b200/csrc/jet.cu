@@ -11,18 +11,27 @@ namespace hp {
 namespace {
 
 constexpr u32 JT = 16;             // thread-level rows up to this degree
-constexpr u32 JW = 512;            // warp-level rows up to this degree
-constexpr u32 JW_SLOTS = 1024;     // per-warp table capacity
+constexpr u32 JW_DEG = 4096;       // warp-level rows up to this degree ...
+constexpr u32 JW_SLOTS = 1024;     // ... whose block table fits this per-warp capacity
 constexpr int JW_BLOCK = 128;      // 4 warps per block
-constexpr u32 JB_SLOTS = 16384;    // per-block table capacity (128 KB)
+constexpr u32 JB_SLOTS = 16384;    // largest per-block table (128 KB)
 constexpr int JB_BLOCK = 512;
-constexpr u32 AB_T = 32;           // afterburner / delta thread-level degree
+constexpr u32 AB_T = 32;           // afterburner / delta: thread-level degree
+constexpr u32 AB_W = 2048;         // afterburner / delta: warp-level degree
 constexpr u32 EMPTY = NO_BLOCK_ID;
 constexpr u32 NOKEY = 0xFFFFFFFFu;
+
+// Block-tier table size: a row never has more distinct blocks than k.
+inline u32 block_slots_for(u32 k) {
+    u32 t = 64;
+    while (t < 2 * k && t < JB_SLOTS) t <<= 1;
+    return t;
+}
 
 struct JArgs {
     DGraph g;
     u32 k;
+    u32 blk_slots;  // block-tier table size (power of two)
     s32 lmax;
     s32 g_weight;
     const u32 *code;     // non-null: process-mapping objective
@@ -287,30 +296,61 @@ __device__ __forceinline__ void count_recompute(const JArgs &a, bool rec, u32 le
     }
 }
 
+// Tier of a row for the table-based kernels: 0 thread, 1 warp, 2 block.
+__device__ __forceinline__ int table_tier(u32 len, u32 k) {
+    if (len <= JT) return 0;
+    const u32 d = len < k ? len : k;
+    return (len <= JW_DEG && 2 * d <= JW_SLOTS) ? 1 : 2;
+}
+
+// Adds per-thread counts to the status word with one atomic per block.
+__device__ __forceinline__ void block_count(u32 *cnt, unsigned long long *sum, u32 c, unsigned long long e) {
+    __shared__ u32 sc[32];
+    __shared__ unsigned long long se[32];
+    c = warp_sum<u32>(c);
+    e = warp_sum<unsigned long long>(e);
+    if (lane_id() == 0) {
+        sc[warp_in_block()] = c;
+        se[warp_in_block()] = e;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        u32 tc = 0;
+        unsigned long long te = 0;
+        for (u32 w = 0; w < (blockDim.x >> 5); ++w) {
+            tc += sc[w];
+            te += se[w];
+        }
+        if (tc && cnt) atomicAdd(cnt, tc);
+        if (te && sum) atomicAdd(sum, te);
+    }
+}
+
 __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
     const u64 stride = (u64) gridDim.x * blockDim.x;
+    u32 nrec = 0;
+    unsigned long long erec = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
         const u32 u = (u32) (base + threadIdx.x);
         int cls = 0;
-        u32 len = 0;
-        bool rec = false;
         if (u < a.g.n) {
             const u32 dc = a.dest_cache[u];
             if (dc != NULL_PART) {
                 a.dest_part[u] = dc;
             } else {
-                rec = true;
-                len = a.g.rowlen[u];
-                if (len <= JT) lp_thread(a, u, ratio);
-                else cls = len <= JW ? 1 : 2;
+                const u32 len = a.g.rowlen[u];
+                ++nrec;
+                erec += len;
+                cls = table_tier(len, a.k);
+                if (cls == 0) lp_thread(a, u, ratio);
             }
         }
-        count_recompute(a, rec, len);
         u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], cls == 1);
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
     }
+    block_count(&a.st->cnt[ST_AUX], (unsigned long long *) &a.st->sum[4], nrec, erec);
 }
 
 __global__ void __launch_bounds__(JW_BLOCK) k_lp_warp(JArgs a, u32 ratio) {
@@ -333,26 +373,28 @@ __global__ void __launch_bounds__(JW_BLOCK) k_lp_warp(JArgs a, u32 ratio) {
 }
 
 __global__ void __launch_bounds__(JB_BLOCK) k_lp_block(JArgs a, u32 ratio) {
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    if (blockIdx.x >= total) return;
     extern __shared__ u32 dsm[];
     u32 *tk = dsm;
-    s32 *tv = (s32 *) (dsm + JB_SLOTS);
+    s32 *tv = (s32 *) (dsm + a.blk_slots);
     __shared__ unsigned long long smu[33];
     __shared__ long long sms[33];
-    for (u32 s = threadIdx.x; s < JB_SLOTS; s += blockDim.x) {
+    for (u32 s = threadIdx.x; s < a.blk_slots; s += blockDim.x) {
         tk[s] = EMPTY;
         tv[s] = 0;
     }
     __syncthreads();
-    const u32 total = a.st->cnt[ST_HEAVY2];
     for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
         const u32 u = a.heavy2[i];
-        const u32 mask = table_mask_for(a.g.rowlen[u], a.k, JB_SLOTS);
+        const u32 mask = table_mask_for(a.g.rowlen[u], a.k, a.blk_slots);
         lp_group<true>(a, u, ratio, tk, tv, mask, smu, sms);
     }
 }
 
 // filter potentially viable moves (:247-258)
-__global__ void k_lp_filter(JArgs a) {
+__global__ void __launch_bounds__(BLOCK) k_lp_filter(JArgs a) {
+    __shared__ u32 sm[33];
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
         const u32 u = (u32) (base + threadIdx.x);
@@ -366,7 +408,7 @@ __global__ void k_lp_filter(JArgs a) {
                 a.lock[u] = 0;
             }
         }
-        const u32 s = warp_append(&a.st->cnt[ST_CAND], c);
+        const u32 s = block_append(&a.st->cnt[ST_CAND], c, sm);
         if (c) a.cand[s] = u;
     }
 }
@@ -385,35 +427,46 @@ __device__ __forceinline__ s32 ab_term(const JArgs &a, u32 u, s32 ug, u32 ou, u3
     return wmul(w, wsub(after_u, before_u));
 }
 
-__global__ void k_ab_thread(JArgs a) {
+// Tier of a row for the neighbour-loop kernels: 0 thread, 1 warp, 2 block.
+__device__ __forceinline__ int loop_tier(u32 len) { return len <= AB_T ? 0 : (len <= AB_W ? 1 : 2); }
+
+// Sum over u's row of the afterburner terms, strided over a group of
+// `nthreads` threads starting at `tid` (wrap-around s32 arithmetic).
+__device__ __forceinline__ s32 ab_partial(const JArgs &a, u32 u, u32 tid, u32 nthreads) {
+    const s32 ug = a.gain1[u];
+    const u32 ou = a.map[u], nu = a.dest_part[u];
+    const u64 beg = a.g.rowptr[u];
+    const u32 len = a.g.rowlen[u];
+    s32 change = 0;
+#pragma unroll 4
+    for (u32 t = tid; t < len; t += nthreads)
+        change = wadd(change, ab_term(a, u, ug, ou, nu, a.g.adj[beg + t], g_ew(a.g, beg + t)));
+    return change;
+}
+
+__global__ void __launch_bounds__(BLOCK) k_ab_thread(JArgs a) {
+    __shared__ u32 sm[33];
     const u32 total = a.st->cnt[ST_CAND];
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
         const u64 i = base + threadIdx.x;
-        bool heavy = false, lock = false;
+        bool lock = false;
+        int tier = -1;
         u32 u = 0;
         if (i < total) {
             u = a.cand[i];
-            const u32 len = a.g.rowlen[u];
-            if (len > AB_T) {
-                heavy = true;
-            } else {
-                const s32 ug = a.gain1[u];
-                const u32 ou = a.map[u], nu = a.dest_part[u];
-                const u64 beg = a.g.rowptr[u];
-                s32 change = 0;
-                for (u32 t = 0; t < len; ++t)
-                    change = wadd(change, ab_term(a, u, ug, ou, nu, a.g.adj[beg + t], g_ew(a.g, beg + t)));
-                if (wadd(ug, change) >= 0) {
-                    a.lock[u] = 1;
-                    lock = true;
-                }
+            tier = loop_tier(a.g.rowlen[u]);
+            if (tier == 0 && wadd(a.gain1[u], ab_partial(a, u, 0, 1)) >= 0) {
+                a.lock[u] = 1;
+                lock = true;
             }
         }
-        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], heavy);
-        if (heavy) a.heavy[s1] = u;
-        const u32 s2 = warp_append(&a.st->cnt[ST_MOVES], lock);
-        if (lock) a.moves[s2] = u;
+        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], tier == 1);
+        if (tier == 1) a.heavy[s1] = u;
+        const u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], tier == 2);
+        if (tier == 2) a.heavy2[s2] = u;
+        const u32 s3 = block_append(&a.st->cnt[ST_MOVES], lock, sm);
+        if (lock) a.moves[s3] = u;
     }
 }
 
@@ -422,15 +475,37 @@ __global__ void k_ab_warp(JArgs a) {
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const u32 u = a.heavy[i];
-        const u32 len = a.g.rowlen[u];
-        const s32 ug = a.gain1[u];
-        const u32 ou = a.map[u], nu = a.dest_part[u];
-        const u64 beg = a.g.rowptr[u];
-        s32 change = 0;
-        for (u32 t = lane_id(); t < len; t += 32)
-            change = wadd(change, ab_term(a, u, ug, ou, nu, a.g.adj[beg + t], g_ew(a.g, beg + t)));
-        change = (s32) warp_sum<u32>((u32) change);
-        if (lane_id() == 0 && wadd(ug, change) >= 0) {
+        const s32 change = (s32) warp_sum<u32>((u32) ab_partial(a, u, lane_id(), 32));
+        if (lane_id() == 0 && wadd(a.gain1[u], change) >= 0) {
+            a.lock[u] = 1;
+            a.moves[atomicAdd(&a.st->cnt[ST_MOVES], 1u)] = u;
+        }
+    }
+}
+
+// Block-wide sum of a u32 (all threads call; result valid in every thread).
+__device__ __forceinline__ u32 block_sum_u32(u32 v, u32 *sm) {
+    v = warp_sum<u32>(v);
+    if (lane_id() == 0) sm[warp_in_block()] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        u32 r = 0;
+        for (u32 w = 0; w < (blockDim.x >> 5); ++w) r += sm[w];
+        sm[32] = r;
+    }
+    __syncthreads();
+    v = sm[32];
+    __syncthreads();
+    return v;
+}
+
+__global__ void __launch_bounds__(JB_BLOCK) k_ab_block(JArgs a) {
+    __shared__ u32 sm[33];
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
+        const u32 u = a.heavy2[i];
+        const s32 change = (s32) block_sum_u32((u32) ab_partial(a, u, threadIdx.x, blockDim.x), sm);
+        if (threadIdx.x == 0 && wadd(a.gain1[u], change) >= 0) {
             a.lock[u] = 1;
             a.moves[atomicAdd(&a.st->cnt[ST_MOVES], 1u)] = u;
         }
@@ -457,68 +532,105 @@ __device__ __forceinline__ long long delta_term(const JArgs &a, u32 ou, u32 nu, 
     return vm ? c : 2 * c;
 }
 
-__global__ void k_delta_thread(JArgs a) {
+// Invalidates the caches of u's neighbours and returns the objective
+// contribution of u's row (strided over a group of threads).
+__device__ __forceinline__ long long delta_partial(const JArgs &a, u32 u, u32 tid, u32 nthreads) {
+    const u64 beg = a.g.rowptr[u];
+    const u32 len = a.g.rowlen[u];
+    const bool um = a.moving[u] == a.epoch;
+    const u32 ou = a.map[u], nu = a.dest_part[u];
+    long long acc = 0;
+#pragma unroll 4
+    for (u32 t = tid; t < len; t += nthreads) {
+        const u32 v = a.g.adj[beg + t];
+        a.dest_cache[v] = NULL_PART;
+        if (um) acc += delta_term(a, ou, nu, v, g_ew(a.g, beg + t));
+    }
+    return acc;
+}
+
+// Adds a per-thread s64 to the status word with one atomic per block.
+__device__ __forceinline__ void block_add_s64(long long v, long long *dst) {
+    __shared__ long long sl[32];
+    v = warp_sum<long long>(v);
+    if (lane_id() == 0) sl[warp_in_block()] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long r = 0;
+        for (u32 w = 0; w < (blockDim.x >> 5); ++w) r += sl[w];
+        if (r) atomicAdd((unsigned long long *) dst, (unsigned long long) r);
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
     const u64 stride = (u64) gridDim.x * blockDim.x;
     long long acc = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
         const u64 i = base + threadIdx.x;
-        bool heavy = false;
+        int tier = -1;
         u32 u = 0;
         if (i < total) {
             u = a.moves[i];
-            const u32 len = a.g.rowlen[u];
-            if (len > AB_T) {
-                heavy = true;
-            } else {
-                const u64 beg = a.g.rowptr[u];
-                const bool um = a.moving[u] == a.epoch;
-                const u32 ou = a.map[u], nu = a.dest_part[u];
-                for (u32 t = 0; t < len; ++t) {
-                    const u32 v = a.g.adj[beg + t];
-                    a.dest_cache[v] = NULL_PART;
-                    if (um) acc += delta_term(a, ou, nu, v, g_ew(a.g, beg + t));
-                }
-            }
+            tier = loop_tier(a.g.rowlen[u]);
+            if (tier == 0) acc += delta_partial(a, u, 0, 1);
         }
-        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY2], heavy);
-        if (heavy) a.heavy2[s1] = u;
+        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], tier == 1);
+        if (tier == 1) a.heavy[s1] = u;
+        const u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], tier == 2);
+        if (tier == 2) a.heavy2[s2] = u;
     }
-    acc = warp_sum<long long>(acc);
-    if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
+    block_add_s64(acc, &a.st->sum[SUM_DELTA]);
 }
 
-__global__ void k_delta_warp(JArgs a) {
-    const u32 total = a.st->cnt[ST_HEAVY2];
+__global__ void __launch_bounds__(BLOCK) k_delta_warp(JArgs a) {
+    const u32 total = a.st->cnt[ST_HEAVY];
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     long long acc = 0;
-    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
-        const u32 u = a.heavy2[i];
-        const u32 len = a.g.rowlen[u];
-        const u64 beg = a.g.rowptr[u];
-        const bool um = a.moving[u] == a.epoch;
-        const u32 ou = a.map[u], nu = a.dest_part[u];
-        for (u32 t = lane_id(); t < len; t += 32) {
-            const u32 v = a.g.adj[beg + t];
-            a.dest_cache[v] = NULL_PART;
-            if (um) acc += delta_term(a, ou, nu, v, g_ew(a.g, beg + t));
-        }
-    }
-    acc = warp_sum<long long>(acc);
-    if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps)
+        acc += delta_partial(a, a.heavy[i], lane_id(), 32);
+    block_add_s64(acc, &a.st->sum[SUM_DELTA]);
 }
 
-__global__ void k_apply(JArgs a) {
+__global__ void __launch_bounds__(JB_BLOCK) k_delta_block(JArgs a) {
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    long long acc = 0;
+    for (u32 i = blockIdx.x; i < total; i += gridDim.x) acc += delta_partial(a, a.heavy2[i], threadIdx.x, blockDim.x);
+    block_add_s64(acc, &a.st->sum[SUM_DELTA]);
+}
+
+constexpr u32 APPLY_SMEM_K = 4096;  // block weights accumulated in shared memory up to this k
+
+__global__ void __launch_bounds__(BLOCK) k_apply(JArgs a) {
+    extern __shared__ s32 sbw[];
     const u32 total = a.st->cnt[ST_MOVES];
+    const bool local = a.k <= APPLY_SMEM_K;
+    if (blockIdx.x * blockDim.x >= total) return;
+    if (local) {
+        for (u32 b = threadIdx.x; b < a.k; b += blockDim.x) sbw[b] = 0;
+        __syncthreads();
+    }
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const u32 u = a.moves[i];
         const u32 ou = a.map[u], nu = a.dest_part[u];
         const s32 w = g_vw(a.g, u);
-        atomicSub(&a.bw[ou], w);
-        atomicAdd(&a.bw[nu], w);
+        if (ou != nu) {
+            if (local) {
+                atomicSub(&sbw[ou], w);
+                atomicAdd(&sbw[nu], w);
+            } else {
+                atomicSub(&a.bw[ou], w);
+                atomicAdd(&a.bw[nu], w);
+            }
+        }
         a.map[u] = nu;
         a.dest_part[u] = ou;
         a.dest_cache[u] = NULL_PART;
+    }
+    if (local) {
+        __syncthreads();
+        for (u32 b = threadIdx.x; b < a.k; b += blockDim.x)
+            if (sbw[b]) atomicAdd(&a.bw[b], sbw[b]);
     }
 }
 
@@ -663,9 +775,8 @@ __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
                 if (!STRONG) a.dest_part[u] = o;
                 r.keys[u] = NOKEY;
             } else {
-                const u32 len = a.g.rowlen[u];
-                if (len <= JT) rb_thread<STRONG>(a, r, u, o);
-                else cls = len <= JW ? 1 : 2;
+                cls = table_tier(a.g.rowlen[u], a.k);
+                if (cls == 0) rb_thread<STRONG>(a, r, u, o);
             }
         }
         u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], cls == 1);
@@ -696,20 +807,21 @@ __global__ void __launch_bounds__(JW_BLOCK) k_rb_warp(JArgs a, RbArgs r) {
 
 template<bool STRONG>
 __global__ void __launch_bounds__(JB_BLOCK) k_rb_block(JArgs a, RbArgs r) {
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    if (blockIdx.x >= total) return;
     extern __shared__ u32 dsm[];
     u32 *tk = dsm;
-    s32 *tv = (s32 *) (dsm + JB_SLOTS);
+    s32 *tv = (s32 *) (dsm + a.blk_slots);
     __shared__ unsigned long long smu[33];
     __shared__ long long sms[33];
-    for (u32 s = threadIdx.x; s < JB_SLOTS; s += blockDim.x) {
+    for (u32 s = threadIdx.x; s < a.blk_slots; s += blockDim.x) {
         tk[s] = EMPTY;
         tv[s] = 0;
     }
     __syncthreads();
-    const u32 total = a.st->cnt[ST_HEAVY2];
     for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
         const u32 u = a.heavy2[i];
-        rb_group<STRONG, true>(a, r, u, tk, tv, table_mask_for(a.g.rowlen[u], a.k, JB_SLOTS), smu, sms);
+        rb_group<STRONG, true>(a, r, u, tk, tv, table_mask_for(a.g.rowlen[u], a.k, a.blk_slots), smu, sms);
     }
 }
 
@@ -941,6 +1053,7 @@ JArgs make_args(JetLevel &L) {
     a.heavy = L.heavy;
     a.heavy2 = L.heavy2;
     a.st = L.ctx->d_status;
+    a.blk_slots = L.blk_slots;
     return a;
 }
 
@@ -1011,7 +1124,7 @@ DistOracle make_dist_oracle(Ctx &ctx, const std::vector<u32> &hier, const std::v
 s64 edge_cut_dev(Ctx &ctx, const DGraph &g, const u32 *part) {
     ctx.zero_counters();
     k_objective<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(
-        g, part, nullptr, nullptr, (unsigned long long *) &ctx.d_status->sum[0]);
+        g, part, nullptr, nullptr, (unsigned long long *) &ctx.d_status->sum[0]); note_launch();
     HP_LAUNCH_CHECK();
     return ctx.read_status().sum[0] / 2;
 }
@@ -1019,20 +1132,20 @@ s64 edge_cut_dev(Ctx &ctx, const DGraph &g, const u32 *part) {
 s64 comm_cost_dev(Ctx &ctx, const DGraph &g, const u32 *part, const DistOracle &D) {
     ctx.zero_counters();
     k_objective<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(
-        g, part, D.code, D.bitdist, (unsigned long long *) &ctx.d_status->sum[0]);
+        g, part, D.code, D.bitdist, (unsigned long long *) &ctx.d_status->sum[0]); note_launch();
     HP_LAUNCH_CHECK();
     return ctx.read_status().sum[0];
 }
 
 void block_weights(Ctx &ctx, const DGraph &g, const u32 *part, u32 k, s32 *bw) {
     HP_CUDA(cudaMemsetAsync(bw, 0, sizeof(s32) * k, ctx.stream));
-    k_block_weights<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, bw);
+    k_block_weights<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, bw); note_launch();
     HP_LAUNCH_CHECK();
 }
 
 s32 max_block_weight(Ctx &ctx, const s32 *bw, u32 k) {
     ctx.zero_counters();
-    k_max_bw<<<1, 1024, 0, ctx.stream>>>(bw, k, &ctx.d_status->imax[MAX_BW]);
+    k_max_bw<<<1, 1024, 0, ctx.stream>>>(bw, k, &ctx.d_status->imax[MAX_BW]); note_launch();
     HP_LAUNCH_CHECK();
     return ctx.read_status().imax[MAX_BW];
 }
@@ -1040,6 +1153,7 @@ s32 max_block_weight(Ctx &ctx, const s32 *bw, u32 k) {
 // ---- JetLevel -----------------------------------------------------------------------
 
 void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle *d, const u32 *part) {
+    ProfScope prof(c, "jet.setup");
     ctx = &c;
     g = gr;
     k = kk;
@@ -1060,6 +1174,7 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     heavy = c.balloc<u32>(n);
     heavy2 = c.balloc<u32>(n);
     epoch = 0;
+    blk_slots = block_slots_for(k);
     HP_CUDA(cudaMemcpyAsync(map, part, sizeof(u32) * n, cudaMemcpyDeviceToDevice, c.stream));
     device_fill<u32>(c, dest_cache, n, NULL_PART);
     HP_CUDA(cudaMemsetAsync(gain_cache, 0, sizeof(s32) * n, c.stream));
@@ -1073,12 +1188,13 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
 
 void JetLevel::gain_pass(u32 ratio_pct) {
     Ctx &c = *ctx;
+    ProfScope prof(c, "jet.gain");
     JArgs a = make_args(*this);
     const u32 n = g.n;
     c.instr.begin(c.stream, "jet_gain", 0.0);
-    k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct);
-    k_lp_warp<<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, ratio_pct);
-    k_lp_block<<<c.sm_count, JB_BLOCK, JB_SLOTS * 8, c.stream>>>(a, ratio_pct);
+    k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
+    k_lp_warp<<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
+    k_lp_block<<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, ratio_pct); note_launch();
     HP_LAUNCH_CHECK();
     c.instr.end(c.stream);
 }
@@ -1087,17 +1203,21 @@ void JetLevel::lp(u32 ratio_pct) {
     Ctx &c = *ctx;
     c.zero_counters();
     gain_pass(ratio_pct);
+    ProfScope prof(c, "jet.filter_afterburner");
     JArgs a = make_args(*this);
     const u32 n = g.n;
-    k_lp_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+    k_lp_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
-    k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
-    k_ab_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
+    k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    k_ab_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    k_ab_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
     HP_LAUNCH_CHECK();
 }
 
 void JetLevel::weak() {
     Ctx &c = *ctx;
+    ProfScope prof(c, "jet.weak");
     const u32 n = g.n;
     const s32 opt = (g_weight + (s32) (k - 1)) / (s32) k;
     s32 max_b_w = (s32) ((99 * (s64) lmax) / 100);
@@ -1108,12 +1228,12 @@ void JetLevel::weak() {
     u32 *under = c.balloc<u32>(k);
     u32 *keys = c.balloc<u32>(n);
     c.zero_counters();
-    k_under<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, under, &c.d_status->cnt[ST_AUX]);
+    k_under<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, under, &c.d_status->cnt[ST_AUX]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, under, keys};
-    k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r);
-    k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r);
-    k_rb_block<false><<<c.sm_count, JB_BLOCK, JB_SLOTS * 8, c.stream>>>(a, r);
+    k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
+    k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+    k_rb_block<false><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
     HP_LAUNCH_CHECK();
     // ordered candidates (ascending id), then a stable sort by mini-bucket key
     u32 *cands = c.balloc<u32>(n);
@@ -1135,14 +1255,15 @@ void JetLevel::weak() {
         c, (u64) cc + 1, [=] __device__(u64 i) -> long long { return i < cc ? (long long) g_vw(gg, cands[i]) : 0; },
         [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr);
     long long *B = c.balloc<long long>((u64) k + 1);
-    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B);
+    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B); note_launch();
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_MOVES], 0, sizeof(u32), c.stream));
-    k_weak_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc);
+    k_weak_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc); note_launch();
     HP_LAUNCH_CHECK();
 }
 
 void JetLevel::strong() {
     Ctx &c = *ctx;
+    ProfScope prof(c, "jet.strong");
     const u32 n = g.n;
     const s32 opt = (g_weight + (s32) (k - 1)) / (s32) k;
     const s32 max_b_w = std::max<s32>(opt + 1, (s32) ((99 * (s64) lmax) / 100));
@@ -1151,12 +1272,12 @@ void JetLevel::strong() {
     ScratchScope ss(c.arena);
     u32 *keys = c.balloc<u32>(n);
     c.zero_counters();
-    k_maxv<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, &c.d_status->imax[1]);
+    k_maxv<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, &c.d_status->imax[1]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, nullptr, keys};
-    k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r);
-    k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r);
-    k_rb_block<true><<<c.sm_count, JB_BLOCK, JB_SLOTS * 8, c.stream>>>(a, r);
+    k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
+    k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+    k_rb_block<true><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
     HP_LAUNCH_CHECK();
     u32 *cands = c.balloc<u32>(n);
     u32 *ck = c.balloc<u32>(n);
@@ -1177,42 +1298,45 @@ void JetLevel::strong() {
         c, (u64) cc + 1, [=] __device__(u64 i) -> long long { return i < cc ? (long long) g_vw(gg, cands[i]) : 0; },
         [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr);
     long long *B = c.balloc<long long>((u64) k + 1);
-    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B);
+    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B); note_launch();
     long long *ea = c.balloc<long long>(k);
     long long *es = c.balloc<long long>((u64) k + 1);
     long long *mpre = c.balloc<long long>((u64) cc + 1);
     HP_CUDA(cudaMemsetAsync(ea, 0, sizeof(long long) * k, c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_MOVES], 0, sizeof(u32), c.stream));
-    k_strong_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc, ea, mpre);
+    k_strong_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc, ea, mpre); note_launch();
     long long *max_v = (long long *) &c.d_status->sum[3];
-    k_cookie<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, B, ea, es, max_v);
+    k_cookie<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, B, ea, es, max_v); note_launch();
     u32 *fail = c.balloc<u32>(n);
     u32 *n_fail = &c.d_status->cnt[ST_HEAVY];
     HP_CUDA(cudaMemsetAsync(n_fail, 0, sizeof(u32), c.stream));
-    k_strong_assign<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, mpre, ea, es, fail, n_fail);
+    k_strong_assign<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, mpre, ea, es, fail, n_fail); note_launch();
     HP_LAUNCH_CHECK();
     const u32 nf = c.read_status().cnt[ST_HEAVY];
     if (nf) {
         u32 *fk = c.balloc<u32>(nf);
         HP_CUDA(cudaMemcpyAsync(fk, fail, sizeof(u32) * nf, cudaMemcpyDeviceToDevice, c.stream));
         radix_sort_pairs<u32>(c, fk, fail, nf, 0, 32);
-        k_strong_fallback<<<1, 32, 0, c.stream>>>(a, fail, nf, es, max_v);
+        k_strong_fallback<<<1, 32, 0, c.stream>>>(a, fail, nf, es, max_v); note_launch();
         HP_LAUNCH_CHECK();
     }
 }
 
 void JetLevel::perform() {
     Ctx &c = *ctx;
+    ProfScope prof(c, "jet.perform");
     ++epoch;
     JArgs a = make_args(*this);
     const u32 n = g.n;
+    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->sum[SUM_DELTA], 0, sizeof(long long), c.stream));
-    k_mark_moving<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
-    k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
-    k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
-    k_apply<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
-    k_max_bw<<<1, 1024, 0, c.stream>>>(bw, k, &c.d_status->imax[MAX_BW]);
+    k_mark_moving<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    k_delta_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+    k_apply<<<c.grid(n, BLOCK), BLOCK, k <= APPLY_SMEM_K ? k * sizeof(s32) : 0, c.stream>>>(a); note_launch();
+    k_max_bw<<<1, 1024, 0, c.stream>>>(bw, k, &c.d_status->imax[MAX_BW]); note_launch();
     HP_LAUNCH_CHECK();
 }
 
@@ -1255,6 +1379,7 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
                 }
             }
             L.perform();
+            ProfScope prof_status(ctx, "jet.status");
             const DevStatus &st = ctx.read_status();
             if (st.err) throw HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
             const u32 nm = st.cnt[ST_MOVES];

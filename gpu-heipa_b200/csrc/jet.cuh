@@ -64,6 +64,7 @@ struct JetLevel {
     u32 *moves = nullptr;
     u32 *heavy = nullptr;
     u32 *heavy2 = nullptr;
+    u32 blk_slots = 0;  // block-tier table size
 
     void setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle *d, const u32 *part);
     // Each of these fills `moves` and leaves the move count in the status

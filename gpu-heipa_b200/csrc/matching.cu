@@ -38,56 +38,101 @@ __device__ __forceinline__ u32 pick_thread(const DGraph &g, const u32 *__restric
     return h;
 }
 
-// Warp version of pick_thread (pick_neighbor_team :143-188 selects the same
-// vertex): lane-local argmax, then a two-step warp reduction.
+// Group version of pick_thread (pick_neighbor_team :143-188 selects the same
+// vertex): every thread of a warp or block keeps the argmax of its strided
+// share of the row, then the group reduces.
+struct PickLocal {
+    bool found;
+    s32 w;
+    u32 tb;
+    u32 h;
+};
+
 template<bool INITIAL>
-__device__ __forceinline__ u32 pick_warp(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed) {
+__device__ __forceinline__ PickLocal pick_local(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed,
+                                                u32 tid, u32 nthreads) {
     const u32 r = xorshift32(u ^ seed);
     const u64 beg = g.rowptr[u];
     const u32 len = g.rowlen[u];
-    u32 h = SENTINEL, tbb = 0;
-    s32 maxw = 0;
-    bool found = false;
-    for (u32 t = lane_id(); t < len; t += 32) {
+    PickLocal p{false, 0, 0, SENTINEL};
+    for (u32 t = tid; t < len; t += nthreads) {
         const u32 v = g.adj[beg + t];
         if (!INITIAL && vcmap[v] != SENTINEL) continue;
         const s32 w = g.ew ? g.ew[beg + t] : 0;
         const u32 tb = xorshift32(v + r);
-        if (!found || w > maxw || (w == maxw && tb >= tbb)) {
-            maxw = w;
-            tbb = tb;
-            h = v;
-            found = true;
-        }
+        if (!p.found || w > p.w || (w == p.w && tb >= p.tb)) p = PickLocal{true, w, tb, v};
     }
-    const s32 wbest = __reduce_max_sync(FULL, found ? maxw : INT32_MIN);
-    if (wbest == INT32_MIN) return SENTINEL;
-    const bool elig = found && maxw == wbest;
-    const u32 tbest = __reduce_max_sync(FULL, elig ? tbb : 0u);
-    const unsigned win = __ballot_sync(FULL, elig && tbb == tbest);
-    return __shfl_sync(FULL, h, __ffs(win) - 1);
+    return p;
 }
 
-__global__ void k_match_init(DGraph g, u32 *vcmap, u32 *hn, u32 seed, u32 *heavy, u32 *heavy_cnt) {
+// Warp argmax of (w, tb); all lanes receive the winner (or an empty pick).
+__device__ __forceinline__ PickLocal pick_reduce_warp(PickLocal p) {
+    const s32 wbest = __reduce_max_sync(FULL, p.found ? p.w : INT32_MIN);
+    if (wbest == INT32_MIN) return PickLocal{false, 0, 0, SENTINEL};
+    const bool elig = p.found && p.w == wbest;
+    const u32 tbest = __reduce_max_sync(FULL, elig ? p.tb : 0u);
+    const unsigned win = __ballot_sync(FULL, elig && p.tb == tbest);
+    return PickLocal{true, wbest, tbest, __shfl_sync(FULL, p.h, __ffs(win) - 1)};
+}
+
+template<bool INITIAL>
+__device__ __forceinline__ u32 pick_warp(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed) {
+    return pick_reduce_warp(pick_local<INITIAL>(g, vcmap, u, seed, lane_id(), 32)).h;
+}
+
+// Block argmax: warp winners go through shared memory to thread 0.
+template<bool INITIAL>
+__device__ __forceinline__ u32 pick_block(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed,
+                                          PickLocal *sm) {
+    PickLocal p = pick_reduce_warp(pick_local<INITIAL>(g, vcmap, u, seed, threadIdx.x, blockDim.x));
+    if (lane_id() == 0) sm[warp_in_block()] = p;
+    __syncthreads();
+    u32 h = SENTINEL;
+    if (threadIdx.x == 0) {
+        PickLocal best{false, 0, 0, SENTINEL};
+        for (u32 w = 0; w < (blockDim.x >> 5); ++w) {
+            const PickLocal q = sm[w];
+            if (q.found && (!best.found || q.w > best.w || (q.w == best.w && q.tb > best.tb))) best = q;
+        }
+        h = best.h;
+    }
+    __syncthreads();
+    return h;
+}
+
+constexpr u32 PICK_WARP_MAX = 4096;  // longer rows are picked by a whole block
+constexpr int PICK_BLOCK = 512;
+
+// Appends u to the warp list (tier 1) or block list (tier 2).
+__device__ __forceinline__ void append_tier(int tier, u32 u, u32 *heavy, u32 *heavy_cnt, u32 *huge, u32 *huge_cnt) {
+    const u32 s1 = warp_append(heavy_cnt, tier == 1);
+    if (tier == 1) heavy[s1] = u;
+    const u32 s2 = warp_append(huge_cnt, tier == 2);
+    if (tier == 2) huge[s2] = u;
+}
+
+__device__ __forceinline__ int pick_tier(u32 len) {
+    return len <= THREAD_DEG_MAX ? 0 : (len <= PICK_WARP_MAX ? 1 : 2);
+}
+
+__global__ void k_match_init(DGraph g, u32 *vcmap, u32 *hn, u32 seed, u32 *heavy, u32 *heavy_cnt, u32 *huge,
+                             u32 *huge_cnt) {
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < g.n; base += stride) {
         const u32 u = (u32) (base + threadIdx.x);
-        bool is_heavy = false;
+        int tier = 0;
         if (u < g.n) {
             vcmap[u] = SENTINEL;
             const u32 len = g.rowlen[u];
             if (!g.ew) {
                 // initial_pick_uniform two_hop_matching.h:279-284
                 hn[u] = len ? g.adj[g.rowptr[u] + (xorshift32(u ^ seed) % len)] : SENTINEL;
-            } else if (len <= THREAD_DEG_MAX) {
-                hn[u] = pick_thread<true>(g, vcmap, u, seed);
             } else {
-                hn[u] = SENTINEL;
-                is_heavy = true;
+                tier = pick_tier(len);
+                hn[u] = tier == 0 ? pick_thread<true>(g, vcmap, u, seed) : SENTINEL;
             }
         }
-        u32 slot = warp_append(heavy_cnt, is_heavy);
-        if (is_heavy) heavy[slot] = u;
+        append_tier(tier, u, heavy, heavy_cnt, huge, huge_cnt);
     }
 }
 
@@ -99,6 +144,18 @@ __global__ void k_pick_heavy(DGraph g, const u32 *vcmap, u32 *hn, u32 seed, cons
         const u32 u = list[i];
         const u32 h = pick_warp<INITIAL>(g, vcmap, u, seed);
         if (lane_id() == 0) hn[u] = h;
+    }
+}
+
+template<bool INITIAL>
+__global__ void __launch_bounds__(PICK_BLOCK) k_pick_huge(DGraph g, const u32 *vcmap, u32 *hn, u32 seed,
+                                                          const u32 *list, const u32 *cnt) {
+    __shared__ PickLocal sm[32];
+    const u32 c = *cnt;
+    for (u32 i = blockIdx.x; i < c; i += gridDim.x) {
+        const u32 u = list[i];
+        const u32 h = pick_block<INITIAL>(g, vcmap, u, seed, sm);
+        if (threadIdx.x == 0) hn[u] = h;
     }
 }
 
@@ -157,22 +214,21 @@ __global__ void k_resolve(const u32 *list, u32 cnt, const u32 *hn, u32 *vcmap, c
 
 // Re-pick for list vertices whose target got matched (:336-374).
 __global__ void k_repick(DGraph g, const u32 *list, u32 cnt, const u32 *vcmap, u32 *hn, u32 seed, u32 *heavy,
-                         u32 *heavy_cnt) {
+                         u32 *heavy_cnt, u32 *huge, u32 *huge_cnt) {
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < cnt; base += stride) {
         const u64 i = base + threadIdx.x;
-        bool is_heavy = false;
+        int tier = 0;
         u32 u = 0;
         if (i < cnt) {
             u = list[i];
             const u32 h = hn[u];
             if (vcmap[u] == SENTINEL && h != SENTINEL && vcmap[h] != SENTINEL) {
-                if (g.rowlen[u] <= THREAD_DEG_MAX) hn[u] = pick_thread<false>(g, vcmap, u, seed);
-                else is_heavy = true;
+                tier = pick_tier(g.rowlen[u]);
+                if (tier == 0) hn[u] = pick_thread<false>(g, vcmap, u, seed);
             }
         }
-        u32 slot = warp_append(heavy_cnt, is_heavy);
-        if (is_heavy) heavy[slot] = u;
+        append_tier(tier, u, heavy, heavy_cnt, huge, huge_cnt);
     }
 }
 
@@ -273,13 +329,13 @@ void pair_by_digest(Ctx &ctx, u32 *cands, K *keys, u32 cnt, u32 *vcmap) {
             if (v) gstart[p] = (u32) i;
         },
         (u32 *) nullptr);
-    k_pair<<<ctx.grid(cnt, BLOCK), BLOCK, 0, ctx.stream>>>(cands, gid, gstart, cnt, vcmap);
+    k_pair<<<ctx.grid(cnt, BLOCK), BLOCK, 0, ctx.stream>>>(cands, gid, gstart, cnt, vcmap); note_launch();
     HP_LAUNCH_CHECK();
 }
 
 u32 count_unmapped(Ctx &ctx, const u32 *vcmap, u32 n) {
     ctx.zero_counters();
-    k_count_unmapped<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, n, &ctx.d_status->cnt[1]);
+    k_count_unmapped<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, n, &ctx.d_status->cnt[1]); note_launch();
     HP_LAUNCH_CHECK();
     return ctx.read_status().cnt[1];
 }
@@ -289,21 +345,26 @@ u32 count_unmapped(Ctx &ctx, const u32 *vcmap, u32 n) {
 u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
     const u32 n = g.n;
     if (n == 0) return 0;
+    ProfScope prof_all(ctx, "match");
     ScratchScope ss(ctx.arena);
     u32 *vcmap = ctx.balloc<u32>(n);
     u32 *hn = ctx.balloc<u32>(n);
     u32 *list = ctx.balloc<u32>(n);
     u32 *list2 = ctx.balloc<u32>(n);
     u32 *heavy = ctx.balloc<u32>(n);
+    u32 *huge = ctx.balloc<u32>(n);
     unsigned long long *claim = ctx.balloc<unsigned long long>(n);
     HP_CUDA(cudaMemsetAsync(claim, 0xFF, sizeof(unsigned long long) * n, ctx.stream));
     u32 *heavy_cnt = &ctx.d_status->cnt[2];
+    u32 *huge_cnt = &ctx.d_status->cnt[3];
+    const u32 hgrid = (u32) ctx.sm_count * 4;
     const u32 seed = MATCH_SEED;
     const u32 wgrid = ctx.grid((u64) n * 32, BLOCK);
 
     ctx.zero_counters();
-    k_match_init<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(g, vcmap, hn, seed, heavy, heavy_cnt);
-    k_pick_heavy<true><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, seed, heavy, heavy_cnt);
+    k_match_init<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(g, vcmap, hn, seed, heavy, heavy_cnt, huge, huge_cnt); note_launch();
+    k_pick_heavy<true><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, seed, heavy, heavy_cnt); note_launch();
+    k_pick_huge<true><<<hgrid, PICK_BLOCK, 0, ctx.stream>>>(g, vcmap, hn, seed, huge, huge_cnt); note_launch();
     device_iota(ctx, list, n);
     HP_LAUNCH_CHECK();
 
@@ -312,16 +373,17 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
     while (cnt > 0) {
         const u32 round_seed = seed ^ (round * 0x9e3779b1u);
         const u32 grid = ctx.grid(cnt, BLOCK);
-        k_mark<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, 0);
+        k_mark<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, 0); note_launch();
         for (u32 r = 0; r < 4; ++r) {
             ++epoch;
             const u32 tag = 0xFFFFFFFFu - epoch;
-            k_claim<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag);
-            k_resolve<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag, r < 3 ? (int) r + 1 : -1);
+            k_claim<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag); note_launch();
+            k_resolve<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag, r < 3 ? (int) r + 1 : -1); note_launch();
         }
         ctx.zero_counters();
-        k_repick<<<grid, BLOCK, 0, ctx.stream>>>(g, list, cnt, vcmap, hn, round_seed, heavy, heavy_cnt);
-        k_pick_heavy<false><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, heavy, heavy_cnt);
+        k_repick<<<grid, BLOCK, 0, ctx.stream>>>(g, list, cnt, vcmap, hn, round_seed, heavy, heavy_cnt, huge, huge_cnt); note_launch();
+        k_pick_heavy<false><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, heavy, heavy_cnt); note_launch();
+        k_pick_huge<false><<<hgrid, PICK_BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, huge, huge_cnt); note_launch();
         HP_LAUNCH_CHECK();
         const u32 *l = list;
         device_select(
@@ -366,7 +428,7 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
         device_select(
             ctx, n, [=] __device__(u64 i) -> bool { return vcmap[i] == SENTINEL; },
             [=] __device__(u64 i) -> u32 { return (u32) i; }, cands, &ctx.d_status->cnt[0]);
-        k_twin_digest<<<wgrid, BLOCK, 0, ctx.stream>>>(g, cands, &ctx.d_status->cnt[0], dig);
+        k_twin_digest<<<wgrid, BLOCK, 0, ctx.stream>>>(g, cands, &ctx.d_status->cnt[0], dig); note_launch();
         HP_LAUNCH_CHECK();
         u32 c = ctx.read_status().cnt[0];
         pair_by_digest<unsigned long long>(ctx, cands, dig, c, vcmap);
@@ -381,13 +443,13 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
         device_select(
             ctx, n, [=] __device__(u64 i) -> bool { return vcmap[i] == SENTINEL; },
             [=] __device__(u64 i) -> u32 { return (u32) i; }, cands, &ctx.d_status->cnt[0]);
-        k_rel_digest<<<wgrid, BLOCK, 0, ctx.stream>>>(g, cands, &ctx.d_status->cnt[0], dig);
+        k_rel_digest<<<wgrid, BLOCK, 0, ctx.stream>>>(g, cands, &ctx.d_status->cnt[0], dig); note_launch();
         HP_LAUNCH_CHECK();
         u32 c = ctx.read_status().cnt[0];
         pair_by_digest<u32>(ctx, cands, dig, c, vcmap);
     }
     // coarse ids (:611-641)
-    k_singletons<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, n);
+    k_singletons<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, n); note_launch();
     HP_LAUNCH_CHECK();
     u32 *rank = list2;
     ctx.zero_counters();
@@ -397,7 +459,7 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
             if (v) rank[i] = p;
         },
         &ctx.d_status->cnt[0]);
-    k_final_map<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, rank, mapping, n);
+    k_final_map<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, rank, mapping, n); note_launch();
     HP_LAUNCH_CHECK();
     return ctx.read_status().cnt[0];
 }

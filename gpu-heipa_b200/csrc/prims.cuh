@@ -99,9 +99,9 @@ void device_scan(Ctx &ctx, u64 n, Load load, Store store, T *total_dev) {
     u64 nt = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (nt == 0) nt = 1;
     T *sums = ctx.balloc<T>(nt);
-    k_scan_reduce<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, load, sums);
-    k_scan_tiles<T><<<1, 1024, 0, ctx.stream>>>(sums, (u32) nt, total_dev);
-    k_scan_apply<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, load, store, sums);
+    k_scan_reduce<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, load, sums); note_launch();
+    k_scan_tiles<T><<<1, 1024, 0, ctx.stream>>>(sums, (u32) nt, total_dev); note_launch();
+    k_scan_apply<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, load, store, sums); note_launch();
     HP_LAUNCH_CHECK();
 }
 
@@ -185,12 +185,12 @@ void radix_sort_pairs(Ctx &ctx, K *keys, u32 *vals, u64 n, int begin_bit, int en
     K *ks = keys, *kd = k_alt;
     u32 *vs = vals, *vd = v_alt;
     for (int shift = begin_bit; shift < end_bit; shift += 8) {
-        k_rs_hist<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, n, shift, hist, ntiles);
+        k_rs_hist<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, n, shift, hist, ntiles); note_launch();
         u64 hn = (u64) 256 * ntiles;
         device_scan<u32>(
             ctx, hn, [=] __device__(u64 i) -> u32 { return hist[i]; },
             [=] __device__(u64 i, u32 p, u32) { hist[i] = p; }, (u32 *) nullptr);
-        k_rs_scatter<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, vs, kd, vd, n, shift, hist, ntiles);
+        k_rs_scatter<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, vs, kd, vd, n, shift, hist, ntiles); note_launch();
         HP_LAUNCH_CHECK();
         std::swap(ks, kd);
         std::swap(vs, vd);
@@ -219,7 +219,7 @@ __global__ void k_fill(T *p, u64 n, T v) {
 template<typename T>
 void device_fill(Ctx &ctx, T *p, u64 n, T v) {
     if (n == 0) return;
-    k_fill<T><<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(p, n, v);
+    k_fill<T><<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(p, n, v); note_launch();
     HP_LAUNCH_CHECK();
 }
 

@@ -81,7 +81,7 @@ void uncoarsen(Ctx &ctx, Hierarchy &H, u32 *coarse_part, u32 *part_out, u32 k, s
         const DGraph &fine = H.graphs[l - 1];
         auto t0 = Clock::now();
         u32 *fpart = (l == 1) ? part_out : ctx.falloc<u32>(fine.n);
-        k_project<<<ctx.grid(fine.n, BLOCK), BLOCK, 0, ctx.stream>>>(cpart, H.maps[l - 1], fpart, fine.n);
+        k_project<<<ctx.grid(fine.n, BLOCK), BLOCK, 0, ctx.stream>>>(cpart, H.maps[l - 1], fpart, fine.n); note_launch();
         HP_LAUNCH_CHECK();
         if (stats) {
             ctx.sync();
@@ -103,13 +103,16 @@ s32 lmax_of(s64 total_weight, u32 k, double eps) {
 }
 
 size_t arena_estimate(u32 n, u64 m, bool has_ew, bool has_vw) {
-    // input graph + hierarchy (about 3x the input rows at worst for the padded
-    // levels) + Jet state (~12 n words) + matching / contraction scratch.
+    // input graph + hierarchy (every padded level holds up to the fine level's
+    // m entries of 8 bytes; power-law graphs keep ~90% of their edges for the
+    // first ~8 levels, so 10 levels' worth are budgeted) + per-level mappings
+    // and Jet state (~60 n words) + matching / contraction scratch (global
+    // hash tables for hub rows).
     const double in = 4.0 * ((double) n + 1) * 2 + 4.0 * (double) m * (has_ew ? 2 : 1) + (has_vw ? 4.0 * n : 0.0);
-    const double hier = 3.0 * (8.0 * (double) m + 16.0 * (double) n);
-    const double scratch = 4.0 * (14.0 * (double) n) + 16.0 * (double) m;
-    const double total = in + hier + scratch + (64ull << 20);
-    return (size_t) (total * 1.15);
+    const double hier = 80.0 * (double) m;
+    const double per_vertex = 240.0 * (double) n;
+    const double scratch = 16.0 * (double) m;
+    return (size_t) (in + hier + per_vertex + scratch + (512.0 * 1024 * 1024));
 }
 
 s64 solve_partition(Ctx &ctx, const DGraph &g, u32 k, double eps, bool ultra, u64 seed, u32 *part,
@@ -129,6 +132,7 @@ s64 solve_partition(Ctx &ctx, const DGraph &g, u32 k, double eps, bool ultra, u6
     const DGraph &coarsest = H.graphs.back();
     // initial partitioning on the host (kway_core.h:1573-1588)
     auto t0 = Clock::now();
+    ProfScope prof_ip(ctx, "initial_partitioning");
     HostCSR hc = download_sorted(ctx, coarsest);
     std::vector<u32> hpart;
     initial_kway(hc, k, eps, seed, hpart);
@@ -172,7 +176,7 @@ void hm_recurse(Ctx &ctx, const DGraph &g, const u32 *n_to_o, const std::vector<
     if (depth == l - 1) {
         u32 offset = 0;
         for (u32 i = 0; i + 1 < l; ++i) offset += identifier[i] * index_vec[index_vec.size() - 1 - i];
-        k_scatter_leaf<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(tmp, n_to_o, g.n, offset, global_part);
+        k_scatter_leaf<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(tmp, n_to_o, g.n, offset, global_part); note_launch();
         HP_LAUNCH_CHECK();
         ctx.sync();
         ctx.arena.front_release(mark);
@@ -188,7 +192,7 @@ void hm_recurse(Ctx &ctx, const DGraph &g, const u32 *n_to_o, const std::vector<
             continue;
         }
         u32 *sub_n_to_o = ctx.falloc<u32>(sub_n);
-        k_compose<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(n_to_o, sub_n_to_o_local, sub_n, sub_n_to_o);
+        k_compose<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(n_to_o, sub_n_to_o_local, sub_n, sub_n_to_o); note_launch();
         HP_LAUNCH_CHECK();
         identifier.push_back(id);
         hm_recurse(ctx, sg, sub_n_to_o, hier, level - 1, identifier, index_vec, k_rem, eps, global_w, global_k, seed,

@@ -65,6 +65,11 @@ _SIG = {
     "hp_last_solve_stats": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "hp_instrument": (_int, [_vp, _int]),
     "hp_kernel_timing": (_int, [_vp, ctypes.c_char_p, _vp, _vp, _vp]),
+    "hp_event_record": (_int, [_vp, _int]),
+    "hp_event_elapsed": (_int, [_vp, _int, _int, _vp]),
+    "hp_kernel_launches": (_u64, []),
+    "hp_profile": (_int, [_vp, _int]),
+    "hp_profile_entry": (_int, [_vp, _u32, ctypes.c_char_p, ctypes.c_size_t, _vp, _vp]),
     "hp_read_metis": (_int, [ctypes.c_char_p, _vp]),
     "hp_gen_grid": (_int, [_u32, _u32, _i32, _i32, _u64, _vp]),
     "hp_gen_rmat": (_int, [_u32, _u32, _dbl, _dbl, _dbl, _i32, _i32, _u64, _int, _vp]),
@@ -164,6 +169,11 @@ class Graph:
         _host_check(_L.hp_gen_rgg3d(n, mean_degree, w_lo, w_hi, seed, int(explicit_vw), ctypes.byref(g)),
                     "rgg generator failed")
         return Graph._from_handle(g)
+
+
+def kernel_launches():
+    """Kernels launched by this process through the library so far."""
+    return int(_L.hp_kernel_launches())
 
 
 def write_partition(path, part):
@@ -367,6 +377,28 @@ class Context:
         self._check(_L.hp_last_solve_stats(self.h, ms, ctypes.byref(o), ctypes.byref(lm), ctypes.byref(lv)))
         keys = ("coarsening", "contraction", "initial_partitioning", "uncontraction", "refinement")
         return dict(phase_ms=dict(zip(keys, list(ms))), initial_obj=o.value, lmax=lm.value, levels=lv.value)
+
+    def event_record(self, slot):
+        self._check(_L.hp_event_record(self.h, int(slot)))
+
+    def event_elapsed(self, a, b):
+        ms = ctypes.c_float()
+        self._check(_L.hp_event_elapsed(self.h, int(a), int(b), ctypes.byref(ms)))
+        return ms.value
+
+    def profile(self, enable=True):
+        """Diagnostic phase timers (synchronising)."""
+        self._check(_L.hp_profile(self.h, int(enable)))
+
+    def profile_entries(self):
+        out = {}
+        i = 0
+        buf = ctypes.create_string_buffer(64)
+        ms, cnt = ctypes.c_double(), _u64()
+        while _L.hp_profile_entry(self.h, i, buf, 64, ctypes.byref(ms), ctypes.byref(cnt)) == 0:
+            out[buf.value.decode()] = (ms.value, cnt.value)
+            i += 1
+        return out
 
     def instrument(self, enable=True):
         self._check(_L.hp_instrument(self.h, int(enable)))

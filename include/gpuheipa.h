@@ -137,6 +137,18 @@ int hp_last_solve_stats(const hp_ctx *ctx, double *phase_ms5, int64_t *initial_o
 int hp_instrument(hp_ctx *ctx, int enable);
 int hp_kernel_timing(hp_ctx *ctx, const char *name, uint64_t *launches, double *ms, double *bytes);
 
+/* Records event `slot` (0..7) on the context's stream; hp_event_elapsed
+ * returns the milliseconds between two recorded slots (synchronises). */
+int hp_event_record(hp_ctx *ctx, int slot);
+int hp_event_elapsed(hp_ctx *ctx, int slot_a, int slot_b, float *ms);
+/* Kernels launched by this process so far. */
+uint64_t hp_kernel_launches(void);
+/* Diagnostic phase timers (synchronising; off by default). hp_profile resets
+ * them; hp_profile_entry enumerates (name, total ms, count) by index and
+ * returns HP_ERR_ARG past the last entry. */
+int hp_profile(hp_ctx *ctx, int enable);
+int hp_profile_entry(const hp_ctx *ctx, uint32_t index, char *name, size_t name_len, double *ms, uint64_t *count);
+
 /* ---- host utilities (no device work) --------------------------------------- */
 
 /* Replaces from_file (src/datastructures/host_graph.h:154-247). */
