@@ -75,8 +75,8 @@ cudaEvent_t Instr::get_event() {
     return e;
 }
 
-void Instr::begin(cudaStream_t s, const char *name, double bytes) {
-    if (!enabled) return;
+size_t Instr::begin(cudaStream_t s, const char *name, double bytes) {
+    if (!enabled) return SIZE_MAX;
     Rec r;
     r.name = name;
     r.a = get_event();
@@ -84,12 +84,19 @@ void Instr::begin(cudaStream_t s, const char *name, double bytes) {
     r.bytes = bytes;
     HP_CUDA(cudaEventRecord(r.a, s));
     pending.push_back(r);
+    return pending.size() - 1;
 }
 
-void Instr::end(cudaStream_t s) {
-    if (!enabled || pending.empty()) return;
-    HP_CUDA(cudaEventRecord(pending.back().b, s));
+void Instr::end(cudaStream_t s, size_t idx) {
+    if (!enabled || idx >= pending.size()) return;
+    HP_CUDA(cudaEventRecord(pending[idx].b, s));
 }
+
+KernTimer::KernTimer(Ctx &ctx, const char *name, double bytes) : c(ctx) {
+    idx = c.instr.begin(c.stream, name, bytes);
+}
+
+KernTimer::~KernTimer() { c.instr.end(c.stream, idx); }
 
 void Instr::resolve() {
     for (Rec &r: pending) {

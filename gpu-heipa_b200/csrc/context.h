@@ -88,8 +88,9 @@ struct Instr {
     std::vector<Total> totals;
     std::vector<cudaEvent_t> pool;
     cudaEvent_t get_event();
-    void begin(cudaStream_t s, const char *name, double bytes);
-    void end(cudaStream_t s);
+    // begin() returns a record index (or SIZE_MAX when disabled) for end().
+    size_t begin(cudaStream_t s, const char *name, double bytes);
+    void end(cudaStream_t s, size_t idx);
     void resolve();  // requires the stream to be idle
     void clear();
     void destroy();
@@ -144,6 +145,15 @@ struct Ctx {
         u64 cap = (u64) sm_count * 16;
         return (u32) (b > cap ? cap : b);
     }
+};
+
+// Records a CUDA-event pair around the launches in a C++ scope when
+// instrumentation is enabled (no synchronisation).
+struct KernTimer {
+    Ctx &c;
+    size_t idx;
+    KernTimer(Ctx &ctx, const char *name, double bytes = 0.0);
+    ~KernTimer();
 };
 
 // RAII scope for PhaseProf.

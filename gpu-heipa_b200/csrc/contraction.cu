@@ -364,38 +364,34 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     ctx.zero_counters();
     DevStatus *st = ctx.d_status;
     CArgs a{g, mapping, moff, mlist, c, &st->err, (unsigned long long *) &st->sum[1]};
-    const size_t rec0 = ctx.instr.pending.size();
-    ctx.instr.begin(ctx.stream, "contract", 0.0);
+    const size_t rec0 = ctx.instr.begin(ctx.stream, "contract", 0.0);
     k_contract_small<<<ctx.grid(n_c, BLOCK), BLOCK, 0, ctx.stream>>>(
         a, wl, &st->cnt[0], bl, &st->cnt[1], hl, &st->cnt[2], hoff, (unsigned long long *) &st->sum[0]); note_launch();
     HP_LAUNCH_CHECK();
-    ctx.instr.end(ctx.stream);
+    ctx.instr.end(ctx.stream, rec0);
     const DevStatus &s1 = ctx.read_status();
     const u32 nw = s1.cnt[0], nb = s1.cnt[1], nh = s1.cnt[2];
     const u64 hslots = (u64) s1.sum[0];
     if (nw) {
-        ctx.instr.begin(ctx.stream, "contract", 0.0);
+        KernTimer kt(ctx, "contract");
         k_contract_warp<<<ctx.grid((u64) nw * 32, C_WARP_BLOCK), C_WARP_BLOCK, 0, ctx.stream>>>(a, wl, &st->cnt[0]); note_launch();
         HP_LAUNCH_CHECK();
-        ctx.instr.end(ctx.stream);
     }
     if (nb) {
         const size_t smem = (size_t) C_BLOCK_SLOTS * 8;
         HP_CUDA(cudaFuncSetAttribute(k_contract_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-        ctx.instr.begin(ctx.stream, "contract", 0.0);
+        KernTimer kt(ctx, "contract");
         k_contract_block<<<(u32) std::min<u64>(nb, (u64) ctx.sm_count * 3), BLOCK, smem, ctx.stream>>>(a, bl,
                                                                                                      &st->cnt[1]); note_launch();
         HP_LAUNCH_CHECK();
-        ctx.instr.end(ctx.stream);
     }
     if (nh) {
         u32 *tkeys = ctx.balloc<u32>(hslots);
         s32 *twts = ctx.balloc<s32>(hslots);
-        ctx.instr.begin(ctx.stream, "contract", 0.0);
+        KernTimer kt(ctx, "contract");
         k_contract_huge<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
             a, hl, &st->cnt[2], hoff, tkeys, twts); note_launch();
         HP_LAUNCH_CHECK();
-        ctx.instr.end(ctx.stream);
     }
     const DevStatus &s2 = ctx.read_status();
     if (s2.err & DEV_ERR_HASH_FULL) throw HpError{HP_ERR_DEVICE, "contraction hash table overflow"};
@@ -403,7 +399,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     // algorithmic bytes of the aggregation pass (roofline accounting): member
     // lists, fine offsets/lengths/weights, fine rows and weights, map gather,
     // coarse rows, weights and lengths
-    if (ctx.instr.enabled && ctx.instr.pending.size() > rec0) {
+    if (rec0 < ctx.instr.pending.size()) {
         const double fine_e = g.ew ? 12.0 : 8.0;
         ctx.instr.pending[rec0].bytes = 12.0 * g.n + fine_e * (double) g.m + 8.0 * n_c + 8.0 * (double) c.m;
     }

@@ -20,6 +20,10 @@ constexpr u32 AB_T = 32;           // afterburner / delta: thread-level degree
 constexpr u32 AB_W = 2048;         // afterburner / delta: warp-level degree
 constexpr u32 EMPTY = NO_BLOCK_ID;
 constexpr u32 NOKEY = 0xFFFFFFFFu;
+// During perform, map[] holds the new label of every vertex and the MOVED
+// bit marks the vertices that changed block in this iteration; their old
+// label is in dest_part[] (the reference's swap, perform_moves :794-795).
+constexpr u32 MOVED = 0x80000000u;
 
 // Block-tier table size: a row never has more distinct blocks than k.
 inline u32 block_slots_for(u32 k) {
@@ -43,7 +47,6 @@ struct JArgs {
     u32 *lock;
     u32 *dest_part;
     s32 *gain1;
-    u32 *moving;
     u32 epoch;
     u32 *cand;
     u32 *moves;
@@ -514,18 +517,20 @@ __global__ void __launch_bounds__(JB_BLOCK) k_ab_block(JArgs a) {
 
 // ---- perform_moves (:753-924 / ProMap :1103-1216) -----------------------------------
 
-__global__ void k_mark_moving(JArgs a) {
+// Clears the MOVED bits set by k_apply once the objective delta is known.
+__global__ void k_unmark(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const u32 u = a.moves[i];
-        if (a.dest_part[u] != a.map[u]) a.moving[u] = a.epoch;
+        a.map[u] &= ~MOVED;
     }
 }
 
 __device__ __forceinline__ long long delta_term(const JArgs &a, u32 ou, u32 nu, u32 v, s32 w) {
-    const u32 ov = a.map[v];
-    const bool vm = a.moving[v] == a.epoch;
-    const u32 nv = vm ? a.dest_part[v] : ov;
+    const u32 x = a.map[v];
+    const bool vm = (x & MOVED) != 0;
+    const u32 nv = x & ~MOVED;
+    const u32 ov = vm ? a.dest_part[v] : nv;
     long long c;
     if (!a.code) c = (long long) w * ((long long) (nu != nv) - (long long) (ou != ov));
     else c = (long long) w * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov));
@@ -537,8 +542,10 @@ __device__ __forceinline__ long long delta_term(const JArgs &a, u32 ou, u32 nu, 
 __device__ __forceinline__ long long delta_partial(const JArgs &a, u32 u, u32 tid, u32 nthreads) {
     const u64 beg = a.g.rowptr[u];
     const u32 len = a.g.rowlen[u];
-    const bool um = a.moving[u] == a.epoch;
-    const u32 ou = a.map[u], nu = a.dest_part[u];
+    const u32 x = a.map[u];
+    const bool um = (x & MOVED) != 0;
+    const u32 nu = x & ~MOVED;
+    const u32 ou = um ? a.dest_part[u] : nu;
     long long acc = 0;
 #pragma unroll 4
     for (u32 t = tid; t < len; t += nthreads) {
@@ -623,7 +630,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(JArgs a) {
                 atomicAdd(&a.bw[nu], w);
             }
         }
-        a.map[u] = nu;
+        a.map[u] = ou != nu ? (nu | MOVED) : nu;
         a.dest_part[u] = ou;
         a.dest_cache[u] = NULL_PART;
     }
@@ -1046,7 +1053,6 @@ JArgs make_args(JetLevel &L) {
     a.lock = L.lock;
     a.dest_part = L.dest_part;
     a.gain1 = L.gain1;
-    a.moving = L.moving;
     a.epoch = L.epoch;
     a.cand = L.cand;
     a.moves = L.moves;
@@ -1168,7 +1174,6 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     lock = c.balloc<u32>(n);
     dest_part = c.balloc<u32>(n);
     gain1 = c.balloc<s32>(n);
-    moving = c.balloc<u32>(n);
     cand = c.balloc<u32>(n);
     moves = c.balloc<u32>(n);
     heavy = c.balloc<u32>(n);
@@ -1179,7 +1184,6 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     device_fill<u32>(c, dest_cache, n, NULL_PART);
     HP_CUDA(cudaMemsetAsync(gain_cache, 0, sizeof(s32) * n, c.stream));
     HP_CUDA(cudaMemsetAsync(lock, 0, sizeof(u32) * n, c.stream));
-    HP_CUDA(cudaMemsetAsync(moving, 0, sizeof(u32) * n, c.stream));
     device_fill<u32>(c, dest_part, n, NO_MOVE);
     HP_CUDA(cudaMemsetAsync(gain1, 0, sizeof(s32) * n, c.stream));
     block_weights(c, g, map, k, bw);
@@ -1191,12 +1195,21 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     ProfScope prof(c, "jet.gain");
     JArgs a = make_args(*this);
     const u32 n = g.n;
-    c.instr.begin(c.stream, "jet_gain", 0.0);
-    k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
-    k_lp_warp<<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
-    k_lp_block<<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, ratio_pct); note_launch();
+    gain_rec = c.instr.begin(c.stream, "jet_gain", 0.0);
+    {
+        KernTimer kt(c, "k_lp_dispatch");
+        k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
+    }
+    {
+        KernTimer kt(c, "k_lp_warp");
+        k_lp_warp<<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
+    }
+    {
+        KernTimer kt(c, "k_lp_block");
+        k_lp_block<<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, ratio_pct); note_launch();
+    }
     HP_LAUNCH_CHECK();
-    c.instr.end(c.stream);
+    c.instr.end(c.stream, gain_rec);
 }
 
 void JetLevel::lp(u32 ratio_pct) {
@@ -1206,9 +1219,13 @@ void JetLevel::lp(u32 ratio_pct) {
     ProfScope prof(c, "jet.filter_afterburner");
     JArgs a = make_args(*this);
     const u32 n = g.n;
-    k_lp_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    {
+        KernTimer kt(c, "k_lp_filter");
+        k_lp_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    }
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
+    KernTimer kt(c, "k_afterburner");
     k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     k_ab_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     k_ab_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
@@ -1231,9 +1248,14 @@ void JetLevel::weak() {
     k_under<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, under, &c.d_status->cnt[ST_AUX]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, under, keys};
-    k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
-    k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
-    k_rb_block<false><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+    {
+        ProfScope p2(c, "weak.pick");
+        KernTimer kt(c, "k_weak_pick");
+        k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
+        k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+        k_rb_block<false><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+    }
+    ProfScope p3(c, "weak.order");
     HP_LAUNCH_CHECK();
     // ordered candidates (ascending id), then a stable sort by mini-bucket key
     u32 *cands = c.balloc<u32>(n);
@@ -1275,9 +1297,14 @@ void JetLevel::strong() {
     k_maxv<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, &c.d_status->imax[1]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, nullptr, keys};
-    k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
-    k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
-    k_rb_block<true><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+    {
+        ProfScope p2(c, "strong.pick");
+        KernTimer kt(c, "k_strong_pick");
+        k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
+        k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+        k_rb_block<true><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+    }
+    ProfScope p3(c, "strong.order");
     HP_LAUNCH_CHECK();
     u32 *cands = c.balloc<u32>(n);
     u32 *ck = c.balloc<u32>(n);
@@ -1331,12 +1358,22 @@ void JetLevel::perform() {
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->sum[SUM_DELTA], 0, sizeof(long long), c.stream));
-    k_mark_moving<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    k_delta_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
-    k_apply<<<c.grid(n, BLOCK), BLOCK, k <= APPLY_SMEM_K ? k * sizeof(s32) : 0, c.stream>>>(a); note_launch();
-    k_max_bw<<<1, 1024, 0, c.stream>>>(bw, k, &c.d_status->imax[MAX_BW]); note_launch();
+    {
+        // labels first (new label + MOVED bit, old label in dest_part) ...
+        ProfScope p2(c, "perform.apply");
+        KernTimer kt(c, "k_apply");
+        k_apply<<<c.grid(n, BLOCK), BLOCK, k <= APPLY_SMEM_K ? k * sizeof(s32) : 0, c.stream>>>(a); note_launch();
+        k_max_bw<<<1, 1024, 0, c.stream>>>(bw, k, &c.d_status->imax[MAX_BW]); note_launch();
+    }
+    {
+        // ... then the exact objective change and the neighbours' cache resets
+        ProfScope p3(c, "perform.delta");
+        KernTimer kt(c, "k_delta");
+        k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        k_delta_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+        k_unmark<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    }
     HP_LAUNCH_CHECK();
 }
 
@@ -1383,6 +1420,15 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
             const DevStatus &st = ctx.read_status();
             if (st.err) throw HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
             const u32 nm = st.cnt[ST_MOVES];
+            if (lp_iter && L.gain_rec < ctx.instr.pending.size()) {
+                // algorithmic bytes of the gain pass: every vertex reads its
+                // cache entry and writes dest_part (8 B); a recomputed vertex
+                // instead reads its offset, length and own label and writes
+                // dest_part and both caches (16 B in all), and each entry of
+                // its row costs adj + ew + the label gather (12 B)
+                const double nrec = st.cnt[ST_AUX], erec = (double) st.sum[4];
+                ctx.instr.pending[L.gain_rec].bytes = 8.0 * (g.n - nrec) + 16.0 * nrec + 12.0 * erec;
+            }
             if (!promap) {
                 if (nm == 0) {
                     if (lp_iter) break;

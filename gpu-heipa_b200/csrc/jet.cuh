@@ -58,13 +58,13 @@ struct JetLevel {
     u32 *lock = nullptr;
     u32 *dest_part = nullptr;
     s32 *gain1 = nullptr;
-    u32 *moving = nullptr;  // epoch stamps of vertices moving in this iteration
     u32 epoch = 0;
     u32 *cand = nullptr;
     u32 *moves = nullptr;
     u32 *heavy = nullptr;
     u32 *heavy2 = nullptr;
     u32 blk_slots = 0;  // block-tier table size
+    size_t gain_rec = SIZE_MAX;  // instrumentation record of the last gain pass
 
     void setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle *d, const u32 *part);
     // Each of these fills `moves` and leaves the move count in the status
