@@ -20,7 +20,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libgpuheipa.so")
 HP_MAP_IM, HP_MAP_HM, HP_MAP_HM_ULTRA = 0, 1, 2
 MAP_MODES = {"IM": HP_MAP_IM, "HM": HP_MAP_HM, "HM-ultra": HP_MAP_HM_ULTRA}
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "I/O error",
-          5: "invalid graph", 6: "device error"}
+          5: "invalid graph", 6: "device error", 7: "input too large"}
+EDGE_CUT_NOALLOC_MAX_N = 4194304
 
 
 class HeiPaError(RuntimeError):
@@ -58,6 +59,7 @@ _SIG = {
     "hp_jet_end": (_int, [_vp]),
     "hp_edge_cut": (_int, [_vp, _vp, _vp, _vp]),
     "hp_comm_cost": (_int, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
+    "hp_edge_cut_noalloc": (_int, [_u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hp_partition": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_partition_graph": (_int, [_vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_map": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
@@ -174,6 +176,23 @@ class Graph:
 def kernel_launches():
     """Kernels launched by this process through the library so far."""
     return int(_L.hp_kernel_launches())
+
+
+def edge_cut_noalloc(n, m, d_xadj, d_adj, d_ew, part, stream=0):
+    """Edge cut of a caller-owned device CSR (integer device addresses of
+    uint32 xadj[n+1], uint32 adj[m] and int32 ew[m] or None) under a host
+    partition, computed without any allocation (hp_edge_cut_noalloc). `stream`
+    is a cudaStream_t handle (0: the legacy default stream). Calls on one
+    device share a fixed scratch area and must not overlap."""
+    part = _a_u32(part)
+    if len(part) != n:
+        raise HeiPaError(1, "partition length differs from n")
+    c = _i64()
+    rc = _L.hp_edge_cut_noalloc(n, m, d_xadj, d_adj, d_ew, _p(part), stream or None, ctypes.byref(c))
+    if rc == 7:
+        raise HeiPaError(rc, f"n = {n} exceeds the limit of {EDGE_CUT_NOALLOC_MAX_N} vertices")
+    _host_check(rc, "edge cut without allocation failed")
+    return c.value
 
 
 def write_partition(path, part):

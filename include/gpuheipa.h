@@ -31,7 +31,8 @@ enum {
     HP_ERR_OOM = 3,
     HP_ERR_IO = 4,
     HP_ERR_GRAPH = 5,
-    HP_ERR_DEVICE = 6
+    HP_ERR_DEVICE = 6,
+    HP_ERR_TOO_LARGE = 7 /* input larger than a fixed-size entry point accepts */
 };
 
 /* Mapping modes for hp_map / hp_map_graph (GPU-HeiProMap --config). */
@@ -107,6 +108,41 @@ int hp_jet_end(hp_jet *jet);
 int hp_edge_cut(hp_ctx *ctx, const hp_graph *g, const uint32_t *part, int64_t *cut);
 int hp_comm_cost(hp_ctx *ctx, const hp_graph *g, const uint32_t *part, const uint32_t *hier, const int32_t *dist,
                  uint32_t levels, int64_t *J);
+
+/* Edge cut without any memory allocation. No counterpart in the reference:
+ * it computes the same objective as hp_edge_cut (edge_cut, src/utility/
+ * edge_cut.h:71-90) for callers that cannot allocate device memory at call
+ * time -- a graph held in another framework's memory pool (a PyTorch tensor, a
+ * serving engine that reserved HBM up front), where cudaMalloc would stall all
+ * streams of the device or fail, and where no hp_ctx (whose arena is sized for
+ * whole solves) exists.
+ *
+ * Inputs: a compact CSR on the current device (d_xadj: n+1 offsets with
+ * d_xadj[n] == m; d_adj: m neighbour ids; d_ew: m weights or NULL for unit
+ * weights), a HOST partition `part` of n labels, and a cudaStream_t (NULL =
+ * the legacy default stream). The call stages `part` in a fixed static device
+ * scratch area of this library (16 MiB + 256 B per device, reserved by the
+ * driver when the library's module is loaded), runs one kernel on `stream`
+ * and waits for that stream before it returns *cut.
+ *
+ * Limits and behaviour:
+ *  - n > HP_EDGE_CUT_NOALLOC_MAX_N returns HP_ERR_TOO_LARGE before any device
+ *    work; use hp_edge_cut for larger graphs.
+ *  - Pointers that are not device memory of the current device return
+ *    HP_ERR_ARG; rows with d_xadj[u+1] < d_xadj[u] or > m, or ids >= n, are
+ *    skipped by the kernel and reported as HP_ERR_GRAPH.
+ *  - The first call on a device resolves the scratch address on that device
+ *    (and loads the module there); make that first call before any stream
+ *    capture begins. Later calls only read a table.
+ *  - The scratch counters are cleared by every call before its kernel; the
+ *    staging area needs no initial value.
+ *  - All calls on one device share the one scratch area: calls that overlap
+ *    (from several host threads, or on streams the caller does not order) race
+ *    and can return wrong results. Serialise them.
+ * No cudaMalloc, cudaFree or allocating library routine is called. */
+#define HP_EDGE_CUT_NOALLOC_MAX_N 4194304u
+int hp_edge_cut_noalloc(uint32_t n, uint32_t m, const uint32_t *d_xadj, const uint32_t *d_adj, const int32_t *d_ew,
+                        const uint32_t *part, void *stream, int64_t *cut);
 
 /* ---- whole solves ---------------------------------------------------------- */
 
