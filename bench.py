@@ -40,9 +40,19 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-heipa_b200"))
 WORKLOADS = {
     "rmat22": dict(kind="rmat", scale=22, ef=16, k=64, desc="R-MAT scale 22, edge factor 16, (0.57,0.19,0.19,0.05), "
                                                           "edge weights U[1,10], k=64, eps=0.03"),
+    "rmat18": dict(kind="rmat", scale=18, ef=16, k=64, desc="R-MAT scale 18, edge factor 16, (0.57,0.19,0.19,0.05), "
+                                                          "edge weights U[1,10], k=64, eps=0.03 (profiling case)"),
     "grid256": dict(kind="grid", w=256, h=256, k=16, desc="2D grid 256x256, unit weights, k=16, eps=0.03"),
 }
 CPU_SAMPLE_SCALE = 18
+# kernel timers with algorithmic byte counts; the roofline reports the one with
+# the largest device time in the timed region
+ROOFLINE_KERNELS = ("contract", "jet_gain", "k_delta")
+# every kernel timer of the library (printed with --kernel-timers)
+KERNEL_TIMERS = ("contract", "jet_gain", "k_lp_dispatch", "k_lp_warp", "k_lp_block", "k_lp_filter", "k_afterburner",
+                 "k_ab_thread", "k_ab_warp", "k_ab_block", "k_apply", "k_delta", "k_delta_thread", "k_delta_warp",
+                 "k_delta_block", "k_weak_pick", "k_weak_dispatch", "k_weak_warp", "k_weak_block", "k_strong_pick",
+                 "k_strong_dispatch", "k_strong_warp", "k_strong_block")
 
 
 def make_graph(H, wl, seed):
@@ -220,7 +230,13 @@ def run_ours(args, world, rank, local):
     ctx.event_record(1)
     ms_total = ctx.event_elapsed(0, 1)
     launches = (H.kernel_launches() - l0) / args.steps
-    timing = {nm: ctx.kernel_timing(nm) for nm in ("contract", "jet_gain")}
+    timing = {nm: ctx.kernel_timing(nm) for nm in ROOFLINE_KERNELS}
+    if args.kernel_timers and rank == 0:
+        for nm in KERNEL_TIMERS:
+            t = ctx.kernel_timing(nm)
+            gbs = t["bytes"] / (t["ms"] / 1e3) / 1e9 if t["ms"] and t["bytes"] else None
+            print(json.dumps({"timer": nm, "ms_per_step": t["ms"] / args.steps,
+                              "launches_per_step": t["launches"] / args.steps, "GB/s": gbs}), file=sys.stderr)
     ctx.instrument(False)
     barrier(world)
     clocks = sampler.stop()
@@ -240,26 +256,27 @@ def run_ours(args, world, rank, local):
         hpart = torch.empty(g.n, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
     except Exception:
         hg, hpart = g, np.empty(g.n, np.uint32)
-    for _ in range(max(1, args.warmup // 2)):
+    e2e_steps = 0 if args.no_e2e else args.steps
+    for _ in range(0 if args.no_e2e else max(1, args.warmup // 2)):
         ctx.partition(hg, k, 0.03, args.config, args.seed, out=hpart)
     barrier(world)
     ctx.event_record(2)
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         ctx.partition(hg, k, 0.03, args.config, args.seed, out=hpart)
     ctx.event_record(3)
-    e2e_ms_total = ctx.event_elapsed(2, 3)
+    e2e_ms_total = ctx.event_elapsed(2, 3) if e2e_steps else 0.0
     barrier(world)
     h2d = 4 * (g.n + 1) + 4 * g.m + (4 * g.m if g.ew is not None else 0) + (4 * g.n if g.vw is not None else 0)
     d2h = 4 * g.n
     ctx.close()
 
-    ms, e2e_ms = reduce_max([ms_total / args.steps, e2e_ms_total / args.steps], world)
+    ms, e2e_ms = reduce_max([ms_total / args.steps, e2e_ms_total / max(1, e2e_steps)], world)
     if rank != 0:
         return 0
     value = world * edges / (ms / 1000.0)
-    e2e_value = world * edges / (e2e_ms / 1000.0)
+    e2e_value = world * edges / (e2e_ms / 1000.0) if e2e_steps else None
     peak, peak_kind = measured_peaks()
-    dom = max(timing, key=lambda x: timing[x]["ms"])
+    dom = max((x for x in timing if timing[x]["bytes"] > 0), key=lambda x: timing[x]["ms"], default="contract")
     t = timing[dom]
     roofline = None
     if t["launches"] and t["ms"] > 0:
@@ -308,6 +325,8 @@ def main():
     ap.add_argument("--config", default="default", choices=["default", "ultra"])
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--kernel-timers", action="store_true", help="print every kernel timer to stderr")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if world > 1:

@@ -617,6 +617,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(JArgs a) {
         for (u32 b = threadIdx.x; b < a.k; b += blockDim.x) sbw[b] = 0;
         __syncthreads();
     }
+    long long entries = 0;
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const u32 u = a.moves[i];
         const u32 ou = a.map[u], nu = a.dest_part[u];
@@ -633,12 +634,15 @@ __global__ void __launch_bounds__(BLOCK) k_apply(JArgs a) {
         a.map[u] = ou != nu ? (nu | MOVED) : nu;
         a.dest_part[u] = ou;
         a.dest_cache[u] = NULL_PART;
+        entries += a.g.rowlen[u];
     }
     if (local) {
         __syncthreads();
         for (u32 b = threadIdx.x; b < a.k; b += blockDim.x)
             if (sbw[b]) atomicAdd(&a.bw[b], sbw[b]);
     }
+    // row entries the delta pass will read (byte accounting of the timers)
+    block_add_s64(entries, &a.st->sum[SUM_PERF_ENTRIES]);
 }
 
 __global__ void k_max_bw(const s32 *bw, u32 k, int *out) {
@@ -1226,9 +1230,18 @@ void JetLevel::lp(u32 ratio_pct) {
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
     KernTimer kt(c, "k_afterburner");
-    k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    k_ab_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    k_ab_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+    {
+        KernTimer kt1(c, "k_ab_thread");
+        k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    }
+    {
+        KernTimer kt1(c, "k_ab_warp");
+        k_ab_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    }
+    {
+        KernTimer kt1(c, "k_ab_block");
+        k_ab_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+    }
     HP_LAUNCH_CHECK();
 }
 
@@ -1251,9 +1264,18 @@ void JetLevel::weak() {
     {
         ProfScope p2(c, "weak.pick");
         KernTimer kt(c, "k_weak_pick");
-        k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
-        k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
-        k_rb_block<false><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+        {
+            KernTimer kt1(c, "k_weak_dispatch");
+            k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
+        }
+        {
+            KernTimer kt1(c, "k_weak_warp");
+            k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+        }
+        {
+            KernTimer kt1(c, "k_weak_block");
+            k_rb_block<false><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+        }
     }
     ProfScope p3(c, "weak.order");
     HP_LAUNCH_CHECK();
@@ -1300,9 +1322,18 @@ void JetLevel::strong() {
     {
         ProfScope p2(c, "strong.pick");
         KernTimer kt(c, "k_strong_pick");
-        k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
-        k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
-        k_rb_block<true><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+        {
+            KernTimer kt1(c, "k_strong_dispatch");
+            k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
+        }
+        {
+            KernTimer kt1(c, "k_strong_warp");
+            k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+        }
+        {
+            KernTimer kt1(c, "k_strong_block");
+            k_rb_block<true><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+        }
     }
     ProfScope p3(c, "strong.order");
     HP_LAUNCH_CHECK();
@@ -1358,6 +1389,7 @@ void JetLevel::perform() {
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->sum[SUM_DELTA], 0, sizeof(long long), c.stream));
+    HP_CUDA(cudaMemsetAsync(&c.d_status->sum[SUM_PERF_ENTRIES], 0, sizeof(long long), c.stream));
     {
         // labels first (new label + MOVED bit, old label in dest_part) ...
         ProfScope p2(c, "perform.apply");
@@ -1369,9 +1401,19 @@ void JetLevel::perform() {
         // ... then the exact objective change and the neighbours' cache resets
         ProfScope p3(c, "perform.delta");
         KernTimer kt(c, "k_delta");
-        k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-        k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-        k_delta_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+        delta_rec = kt.idx;
+        {
+            KernTimer kt1(c, "k_delta_thread");
+            k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        }
+        {
+            KernTimer kt1(c, "k_delta_warp");
+            k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        }
+        {
+            KernTimer kt1(c, "k_delta_block");
+            k_delta_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+        }
         k_unmark<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }
     HP_LAUNCH_CHECK();
@@ -1428,6 +1470,15 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
                 // its row costs adj + ew + the label gather (12 B)
                 const double nrec = st.cnt[ST_AUX], erec = (double) st.sum[4];
                 ctx.instr.pending[L.gain_rec].bytes = 8.0 * (g.n - nrec) + 16.0 * nrec + 12.0 * erec;
+            }
+            if (L.delta_rec < ctx.instr.pending.size()) {
+                // algorithmic bytes of the delta pass (all tiers and the
+                // unmark pass): per move its list entry, offset, length, label
+                // and old label and the unmark read-modify-write (36 B); per
+                // entry of a moved row adj (+ ew), the neighbour's label and
+                // its cache reset
+                const double ent = (double) st.sum[SUM_PERF_ENTRIES];
+                ctx.instr.pending[L.delta_rec].bytes = 36.0 * nm + (g.ew ? 16.0 : 12.0) * ent;
             }
             if (!promap) {
                 if (nm == 0) {

@@ -64,7 +64,8 @@ struct JetLevel {
     u32 *heavy = nullptr;
     u32 *heavy2 = nullptr;
     u32 blk_slots = 0;  // block-tier table size
-    size_t gain_rec = SIZE_MAX;  // instrumentation record of the last gain pass
+    size_t gain_rec = SIZE_MAX;   // instrumentation record of the last gain pass
+    size_t delta_rec = SIZE_MAX;  // instrumentation record of the last delta pass
 
     void setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle *d, const u32 *part);
     // Each of these fills `moves` and leaves the move count in the status
@@ -87,6 +88,7 @@ constexpr int ST_CAND = 5;
 constexpr int ST_HEAVY2 = 6;
 constexpr int ST_AUX = 7;
 constexpr int SUM_DELTA = 2;
+constexpr int SUM_PERF_ENTRIES = 5;  // row entries of the moved vertices (perform)
 constexpr int MAX_BW = 0;
 
 // jet_refine (jet_label_propagation.h:926-1033) / ProMap_jet_refine
