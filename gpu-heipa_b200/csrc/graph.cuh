@@ -25,7 +25,7 @@ struct DGraph {
     s64 total_vw = 0;
 };
 
-__device__ __forceinline__ s32 g_ew(const DGraph &g, u64 j) { return g.ew ? g.ew[j] : 1; }
+__device__ __forceinline__ s32 g_ew(const DGraph &g, u64 j) { return g.ew ? __ldg(&g.ew[j]) : 1; }
 __device__ __forceinline__ s32 g_vw(const DGraph &g, u32 u) { return g.vw ? g.vw[u] : 1; }
 
 // Uploads a host CSR (xadj n+1, adj m, optional ew/vw) into the front of the

@@ -52,6 +52,8 @@ struct JArgs {
     u32 *moves;
     u32 *heavy;
     u32 *heavy2;
+    unsigned long long *items;  // delta pass work items: (vertex << 32) | chunk
+    u32 items_cap;
     DevStatus *st;
 };
 
@@ -111,26 +113,42 @@ __device__ __forceinline__ u32 table_mask_for(u32 len, u32 k, u32 cap) {
     return t - 1;
 }
 
-// Aggregates conn(u, .) into the group's table (cleared on entry).
+// Aggregates conn(u, .) into the group's hashed table (cleared on entry).
+// Four entries per thread are loaded before they are inserted.
 template<bool BLK>
 __device__ __forceinline__ void table_build(const JArgs &a, u32 u, u32 *tk, s32 *tv, u32 mask) {
-    const u64 beg = a.g.rowptr[u];
-    const u32 len = a.g.rowlen[u];
-    for (u32 t = Grp<BLK>::tid(); t < len; t += Grp<BLK>::size()) {
-        const u32 b = a.map[a.g.adj[beg + t]];
-        const s32 w = g_ew(a.g, beg + t);
-        u32 h = thash(b, mask);
-        bool ok = false;
-        for (u32 p = 0; p <= mask; ++p) {
-            const u32 prev = atomicCAS(&tk[h], EMPTY, b);
-            if (prev == EMPTY || prev == b) {
-                atomicAdd(&tv[h], w);
-                ok = true;
-                break;
-            }
-            h = (h + 1) & mask;
+    const u64 beg = __ldg(&a.g.rowptr[u]);
+    const u32 len = __ldg(&a.g.rowlen[u]);
+    const u32 gs = Grp<BLK>::size();
+    for (u32 t0 = Grp<BLK>::tid(); t0 < len; t0 += 4 * gs) {
+        u32 bb[4];
+        s32 ww[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u32 t = t0 + j * gs;
+            bb[j] = t < len ? __ldg(&a.g.adj[beg + t]) : EMPTY;
+            ww[j] = t < len ? g_ew(a.g, beg + t) : 0;
         }
-        if (!ok) set_error(&a.st->err, DEV_ERR_HASH_FULL);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (bb[j] != EMPTY) bb[j] = __ldg(&a.map[bb[j]]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u32 b = bb[j];
+            if (b == EMPTY) continue;
+            u32 h = thash(b, mask);
+            bool ok = false;
+            for (u32 p = 0; p <= mask; ++p) {
+                const u32 prev = atomicCAS(&tk[h], EMPTY, b);
+                if (prev == EMPTY || prev == b) {
+                    atomicAdd(&tv[h], ww[j]);
+                    ok = true;
+                    break;
+                }
+                h = (h + 1) & mask;
+            }
+            if (!ok) set_error(&a.st->err, DEV_ERR_HASH_FULL);
+        }
     }
     Grp<BLK>::sync();
 }
@@ -144,6 +162,61 @@ __device__ __forceinline__ void table_clear(u32 *tk, s32 *tv, u32 mask) {
     }
     Grp<BLK>::sync();
 }
+
+// Direct-indexed variant for small k: tv[b] = conn(u, b) for b < k (0 = no
+// connection; weights are positive), so an entry costs one shared-memory add
+// and no compare-and-swap. Four entries per thread are loaded (ids, then
+// labels) before any table update, which keeps four gathers in flight.
+template<bool BLK>
+__device__ __forceinline__ void dtable_build(const JArgs &a, u32 u, s32 *tv) {
+    const u64 beg = __ldg(&a.g.rowptr[u]);
+    const u32 len = __ldg(&a.g.rowlen[u]);
+    const u32 gs = Grp<BLK>::size(), tid = Grp<BLK>::tid();
+    for (u32 t0 = tid; t0 < len; t0 += 4 * gs) {
+        u32 b[4];
+        s32 w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u32 t = t0 + j * gs;
+            b[j] = t < len ? __ldg(&a.g.adj[beg + t]) : EMPTY;
+            w[j] = t < len ? g_ew(a.g, beg + t) : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (b[j] != EMPTY) b[j] = __ldg(&a.map[b[j]]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (b[j] != EMPTY) atomicAdd(&tv[b[j]], w[j]);
+    }
+    Grp<BLK>::sync();
+}
+
+template<bool BLK>
+__device__ __forceinline__ void dtable_clear(s32 *tv, u32 k) {
+    Grp<BLK>::sync();
+    for (u32 s = Grp<BLK>::tid(); s < k; s += Grp<BLK>::size()) tv[s] = 0;
+    Grp<BLK>::sync();
+}
+
+// Connectivity table of one row: direct-indexed (DIRECT) or hashed.
+template<bool BLK, bool DIRECT>
+struct ConnTable {
+    u32 *tk;
+    s32 *tv;
+    u32 mask;  // hashed: slots - 1
+    u32 k;
+    __device__ __forceinline__ void build(const JArgs &a, u32 u) {
+        if (DIRECT) dtable_build<BLK>(a, u, tv);
+        else table_build<BLK>(a, u, tk, tv, mask);
+    }
+    __device__ __forceinline__ u32 slots() const { return DIRECT ? k : mask + 1; }
+    __device__ __forceinline__ u32 key(u32 s) const { return DIRECT ? (tv[s] != 0 ? s : EMPTY) : tk[s]; }
+    __device__ __forceinline__ s32 val(u32 s) const { return tv[s]; }
+    __device__ __forceinline__ void clear() {
+        if (DIRECT) dtable_clear<BLK>(tv, k);
+        else table_clear<BLK>(tk, tv, mask);
+    }
+};
 
 // Thread-level connectivity row in registers (degree <= JT).
 struct TRow {
@@ -252,28 +325,29 @@ __device__ __forceinline__ void lp_thread(const JArgs &a, u32 u, u32 ratio) {
     }
 }
 
-template<bool BLK>
-__device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, u32 *tk, s32 *tv, u32 mask,
+template<bool BLK, bool DIRECT>
+__device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT> T,
                                          unsigned long long *smu, long long *sms) {
-    table_build<BLK>(a, u, tk, tv, mask);
+    T.build(a, u);
     const u32 o = a.map[u];
     unsigned long long bk = 0;
     long long own = 0;
-    for (u32 s = Grp<BLK>::tid(); s <= mask; s += Grp<BLK>::size()) {
-        const u32 b = tk[s];
+    const u32 ns = T.slots();
+    for (u32 s = Grp<BLK>::tid(); s < ns; s += Grp<BLK>::size()) {
+        const u32 b = T.key(s);
         if (b == EMPTY) continue;
         if (b == o) {
-            own = tv[s];
+            own = T.val(s);
             continue;
         }
         unsigned long long k;
         if (!a.code) {
-            k = cut_key(tv[s], b);
+            k = cut_key(T.val(s), b);
         } else {
             s32 d = 0;
-            for (u32 t = 0; t <= mask; ++t) {
-                const u32 id = tk[t];
-                if (id != EMPTY) d = wadd(d, wmul(tv[t], wsub(D(a, o, id), D(a, b, id))));
+            for (u32 t = 0; t < ns; ++t) {
+                const u32 id = T.key(t);
+                if (id != EMPTY) d = wadd(d, wmul(T.val(t), wsub(D(a, o, id), D(a, b, id))));
             }
             k = delta_key(d, b);
         }
@@ -285,7 +359,13 @@ __device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, u32 *
         if (!a.code) lp_finish_cut(a, u, (s32) own, bk, ratio);
         else lp_finish_map(a, u, bk);
     }
-    table_clear<BLK>(tk, tv, mask);
+    T.clear();
+}
+
+// Direct-indexed tables are used when k fits the table and, for the mapping
+// objective (whose candidate scoring loops over the whole table), k is small.
+__device__ __forceinline__ bool use_direct(const JArgs &a, u32 cap) {
+    return a.k <= cap && (!a.code || a.k <= 256);
 }
 
 // Counts recomputed vertices / entries for roofline accounting.
@@ -356,22 +436,29 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
     block_count(&a.st->cnt[ST_AUX], (unsigned long long *) &a.st->sum[4], nrec, erec);
 }
 
-__global__ void __launch_bounds__(JW_BLOCK) k_lp_warp(JArgs a, u32 ratio) {
-    __shared__ u32 tk_all[JW_BLOCK / 32][JW_SLOTS];
-    __shared__ s32 tv_all[JW_BLOCK / 32][JW_SLOTS];
-    u32 *tk = tk_all[warp_in_block()];
-    s32 *tv = tv_all[warp_in_block()];
-    for (u32 s = lane_id(); s < JW_SLOTS; s += 32) {
-        tk[s] = EMPTY;
-        tv[s] = 0;
-    }
+// Per-warp shared memory of the warp-tier kernels (dynamic, sized by the
+// host): a direct-indexed table of wslots >= k values, or a hashed table of
+// wslots keys followed by wslots values.
+template<bool DIRECT>
+__device__ __forceinline__ u32 *warp_table(u32 wslots) {
+    extern __shared__ u32 dsm[];
+    u32 *w = dsm + warp_in_block() * (DIRECT ? wslots : 2 * wslots);
+    for (u32 s = lane_id(); s < (DIRECT ? wslots : 2 * wslots); s += 32) w[s] = (!DIRECT && s < wslots) ? EMPTY : 0u;
     __syncwarp();
+    return w;
+}
+
+template<bool DIRECT>
+__global__ void __launch_bounds__(JW_BLOCK) k_lp_warp(JArgs a, u32 ratio, u32 wslots) {
+    u32 *w = warp_table<DIRECT>(wslots);
+    u32 *tk = w;
+    s32 *tv = (s32 *) (DIRECT ? w : w + wslots);
     const u32 total = a.st->cnt[ST_HEAVY];
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const u32 u = a.heavy[i];
-        const u32 mask = table_mask_for(a.g.rowlen[u], a.k, JW_SLOTS);
-        lp_group<false>(a, u, ratio, tk, tv, mask, nullptr, nullptr);
+        const u32 mask = DIRECT ? 0u : table_mask_for(a.g.rowlen[u], a.k, wslots);
+        lp_group<false, DIRECT>(a, u, ratio, ConnTable<false, DIRECT>{tk, tv, mask, a.k}, nullptr, nullptr);
     }
 }
 
@@ -388,10 +475,12 @@ __global__ void __launch_bounds__(JB_BLOCK) k_lp_block(JArgs a, u32 ratio) {
         tv[s] = 0;
     }
     __syncthreads();
+    const bool direct = use_direct(a, a.blk_slots);
     for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
         const u32 u = a.heavy2[i];
         const u32 mask = table_mask_for(a.g.rowlen[u], a.k, a.blk_slots);
-        lp_group<true>(a, u, ratio, tk, tv, mask, smu, sms);
+        if (direct) lp_group<true, true>(a, u, ratio, ConnTable<true, true>{tk, tv, mask, a.k}, smu, sms);
+        else lp_group<true, false>(a, u, ratio, ConnTable<true, false>{tk, tv, mask, a.k}, smu, sms);
     }
 }
 
@@ -526,32 +615,47 @@ __global__ void k_unmark(JArgs a) {
     }
 }
 
-__device__ __forceinline__ long long delta_term(const JArgs &a, u32 ou, u32 nu, u32 v, s32 w) {
-    const u32 x = a.map[v];
-    const bool vm = (x & MOVED) != 0;
-    const u32 nv = x & ~MOVED;
-    const u32 ov = vm ? a.dest_part[v] : nv;
-    long long c;
-    if (!a.code) c = (long long) w * ((long long) (nu != nv) - (long long) (ou != ov));
-    else c = (long long) w * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov));
-    return vm ? c : 2 * c;
-}
 
-// Invalidates the caches of u's neighbours and returns the objective
-// contribution of u's row (strided over a group of threads).
-__device__ __forceinline__ long long delta_partial(const JArgs &a, u32 u, u32 tid, u32 nthreads) {
-    const u64 beg = a.g.rowptr[u];
-    const u32 len = a.g.rowlen[u];
-    const u32 x = a.map[u];
+// Invalidates the caches of the neighbours in entries [from, to) of u's row
+// and returns their objective contribution (strided over a group of threads).
+// Labels and old labels are not written while the delta kernels run, so they
+// are read through the non-coherent path; four entries per thread are loaded
+// (ids, then labels, then old labels of moved neighbours) before the cache
+// resets are stored, which keeps four dependent gathers in flight.
+__device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 nthreads) {
+    const u64 beg = __ldg(&a.g.rowptr[u]);
+    const u32 x = __ldg(&a.map[u]);
     const bool um = (x & MOVED) != 0;
     const u32 nu = x & ~MOVED;
-    const u32 ou = um ? a.dest_part[u] : nu;
+    const u32 ou = um ? __ldg(&a.dest_part[u]) : nu;
     long long acc = 0;
-#pragma unroll 4
-    for (u32 t = tid; t < len; t += nthreads) {
-        const u32 v = a.g.adj[beg + t];
-        a.dest_cache[v] = NULL_PART;
-        if (um) acc += delta_term(a, ou, nu, v, g_ew(a.g, beg + t));
+    for (u32 t0 = from + tid; t0 < to; t0 += 4 * nthreads) {
+        u32 v[4], xv[4], ov[4];
+        s32 w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u32 t = t0 + j * nthreads;
+            v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
+            w[j] = t < to ? g_ew(a.g, beg + t) : 0;
+        }
+        if (um) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) xv[j] = v[j] != SENTINEL ? __ldg(&a.map[v[j]]) : 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) ov[j] = (xv[j] & MOVED) ? __ldg(&a.dest_part[v[j]]) : (xv[j] & ~MOVED);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (v[j] == SENTINEL) continue;
+                const u32 nv = xv[j] & ~MOVED;
+                long long c;
+                if (!a.code) c = (long long) w[j] * ((long long) (nu != nv) - (long long) (ou != ov[j]));
+                else c = (long long) w[j] * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov[j]));
+                acc += (xv[j] & MOVED) ? c : 2 * c;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (v[j] != SENTINEL) a.dest_cache[v[j]] = NULL_PART;
     }
     return acc;
 }
@@ -569,40 +673,58 @@ __device__ __forceinline__ void block_add_s64(long long v, long long *dst) {
     }
 }
 
+// Rows of moved vertices up to DELTA_THREAD_MAX entries are handled by one
+// thread; longer rows are cut into chunks of DELTA_CHUNK entries, one warp per
+// chunk, so that hub rows spread over the whole GPU instead of one block.
+constexpr u32 DELTA_THREAD_MAX = 32;
+constexpr u32 DELTA_CHUNK = 1024;
+
 __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
     const u64 stride = (u64) gridDim.x * blockDim.x;
     long long acc = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
         const u64 i = base + threadIdx.x;
-        int tier = -1;
-        u32 u = 0;
+        u32 u = 0, nch = 0;
         if (i < total) {
             u = a.moves[i];
-            tier = loop_tier(a.g.rowlen[u]);
-            if (tier == 0) acc += delta_partial(a, u, 0, 1);
+            const u32 len = a.g.rowlen[u];
+            if (len <= DELTA_THREAD_MAX) acc += delta_range(a, u, 0, len, 0, 1);
+            else nch = (len + DELTA_CHUNK - 1) / DELTA_CHUNK;
         }
-        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], tier == 1);
-        if (tier == 1) a.heavy[s1] = u;
-        const u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], tier == 2);
-        if (tier == 2) a.heavy2[s2] = u;
+        // warp-aggregated reservation of the chunk items
+        u32 incl = nch;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(FULL, incl, o);
+            if (lane_id() >= o) incl += y;
+        }
+        const u32 wtot = __shfl_sync(FULL, incl, 31);
+        u32 wbase = 0;
+        if (lane_id() == 31 && wtot) wbase = atomicAdd(&a.st->cnt[ST_HEAVY], wtot);
+        wbase = __shfl_sync(FULL, wbase, 31);
+        const u32 first = wbase + incl - nch;
+        for (u32 c = 0; c < nch; ++c) {
+            if (first + c < a.items_cap) a.items[first + c] = ((unsigned long long) u << 32) | c;
+            else set_error(&a.st->err, DEV_ERR_RANGE);
+        }
     }
     block_add_s64(acc, &a.st->sum[SUM_DELTA]);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_delta_warp(JArgs a) {
-    const u32 total = a.st->cnt[ST_HEAVY];
+__global__ void __launch_bounds__(BLOCK) k_delta_chunk(JArgs a) {
+    u32 total = a.st->cnt[ST_HEAVY];
+    if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     long long acc = 0;
-    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps)
-        acc += delta_partial(a, a.heavy[i], lane_id(), 32);
-    block_add_s64(acc, &a.st->sum[SUM_DELTA]);
-}
-
-__global__ void __launch_bounds__(JB_BLOCK) k_delta_block(JArgs a) {
-    const u32 total = a.st->cnt[ST_HEAVY2];
-    long long acc = 0;
-    for (u32 i = blockIdx.x; i < total; i += gridDim.x) acc += delta_partial(a, a.heavy2[i], threadIdx.x, blockDim.x);
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const unsigned long long it = a.items[i];
+        const u32 u = (u32) (it >> 32);
+        const u32 from = (u32) it * DELTA_CHUNK;
+        const u32 len = a.g.rowlen[u];
+        const u32 to = len - from < DELTA_CHUNK ? len : from + DELTA_CHUNK;
+        acc += delta_range(a, u, from, to, lane_id(), 32);
+    }
     block_add_s64(acc, &a.st->sum[SUM_DELTA]);
 }
 
@@ -734,26 +856,27 @@ __device__ __forceinline__ void rb_thread(const JArgs &a, const RbArgs &r, u32 u
     else weak_finish(a, r, u, o, own, bk);
 }
 
-template<bool STRONG, bool BLK>
-__device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u, u32 *tk, s32 *tv, u32 mask,
+template<bool STRONG, bool BLK, bool DIRECT>
+__device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u, ConnTable<BLK, DIRECT> T,
                                          unsigned long long *smu, long long *sms) {
-    table_build<BLK>(a, u, tk, tv, mask);
+    T.build(a, u);
     const u32 o = a.map[u];
     long long own = 0, sum = 0, count = 0;
     unsigned long long bk = 0;
-    for (u32 s = Grp<BLK>::tid(); s <= mask; s += Grp<BLK>::size()) {
-        const u32 b = tk[s];
+    const u32 ns = T.slots();
+    for (u32 s = Grp<BLK>::tid(); s < ns; s += Grp<BLK>::size()) {
+        const u32 b = T.key(s);
         if (b == EMPTY) continue;
         if (b == o) {
-            own = tv[s];
+            own = T.val(s);
             continue;
         }
         if (a.bw[b] < r.max_b_w) {
             if (STRONG) {
-                sum = (long long) wadd((s32) sum, tv[s]);
+                sum = (long long) wadd((s32) sum, T.val(s));
                 ++count;
             } else {
-                unsigned long long k = cut_key(tv[s], b);
+                unsigned long long k = cut_key(T.val(s), b);
                 bk = k > bk ? k : bk;
             }
         }
@@ -770,7 +893,7 @@ __device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u,
         if (STRONG) strong_finish(a, r, u, o, (s32) own, (s32) sum, (s32) count);
         else weak_finish(a, r, u, o, (s32) own, bk);
     }
-    table_clear<BLK>(tk, tv, mask);
+    T.clear();
 }
 
 template<bool STRONG>
@@ -797,22 +920,17 @@ __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
     }
 }
 
-template<bool STRONG>
-__global__ void __launch_bounds__(JW_BLOCK) k_rb_warp(JArgs a, RbArgs r) {
-    __shared__ u32 tk_all[JW_BLOCK / 32][JW_SLOTS];
-    __shared__ s32 tv_all[JW_BLOCK / 32][JW_SLOTS];
-    u32 *tk = tk_all[warp_in_block()];
-    s32 *tv = tv_all[warp_in_block()];
-    for (u32 s = lane_id(); s < JW_SLOTS; s += 32) {
-        tk[s] = EMPTY;
-        tv[s] = 0;
-    }
-    __syncwarp();
+template<bool STRONG, bool DIRECT>
+__global__ void __launch_bounds__(JW_BLOCK) k_rb_warp(JArgs a, RbArgs r, u32 wslots) {
+    u32 *w = warp_table<DIRECT>(wslots);
+    u32 *tk = w;
+    s32 *tv = (s32 *) (DIRECT ? w : w + wslots);
     const u32 total = a.st->cnt[ST_HEAVY];
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const u32 u = a.heavy[i];
-        rb_group<STRONG, false>(a, r, u, tk, tv, table_mask_for(a.g.rowlen[u], a.k, JW_SLOTS), nullptr, nullptr);
+        const u32 mask = DIRECT ? 0u : table_mask_for(a.g.rowlen[u], a.k, wslots);
+        rb_group<STRONG, false, DIRECT>(a, r, u, ConnTable<false, DIRECT>{tk, tv, mask, a.k}, nullptr, nullptr);
     }
 }
 
@@ -830,9 +948,12 @@ __global__ void __launch_bounds__(JB_BLOCK) k_rb_block(JArgs a, RbArgs r) {
         tv[s] = 0;
     }
     __syncthreads();
+    const bool direct = use_direct(a, a.blk_slots);
     for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
         const u32 u = a.heavy2[i];
-        rb_group<STRONG, true>(a, r, u, tk, tv, table_mask_for(a.g.rowlen[u], a.k, a.blk_slots), smu, sms);
+        const u32 mask = table_mask_for(a.g.rowlen[u], a.k, a.blk_slots);
+        if (direct) rb_group<STRONG, true, true>(a, r, u, ConnTable<true, true>{tk, tv, mask, a.k}, smu, sms);
+        else rb_group<STRONG, true, false>(a, r, u, ConnTable<true, false>{tk, tv, mask, a.k}, smu, sms);
     }
 }
 
@@ -1062,6 +1183,8 @@ JArgs make_args(JetLevel &L) {
     a.moves = L.moves;
     a.heavy = L.heavy;
     a.heavy2 = L.heavy2;
+    a.items = L.items;
+    a.items_cap = L.items_cap;
     a.st = L.ctx->d_status;
     a.blk_slots = L.blk_slots;
     return a;
@@ -1182,8 +1305,18 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     moves = c.balloc<u32>(n);
     heavy = c.balloc<u32>(n);
     heavy2 = c.balloc<u32>(n);
+    // chunk items of the delta pass: one per row of <= DELTA_CHUNK entries,
+    // so at most n + m / DELTA_CHUNK + 1
+    items_cap = (u32) std::min<u64>(0xFFFFFFFFull, (u64) n + g.m / DELTA_CHUNK + 1);
+    items = c.balloc<unsigned long long>(items_cap);
     epoch = 0;
     blk_slots = block_slots_for(k);
+    // warp tier: direct-indexed table of k values when k is small enough
+    // (for the mapping objective the candidate scoring loops over the table,
+    // so only up to 256 blocks), else a hashed table of JW_SLOTS slots
+    warp_direct = k <= JW_SLOTS && (d == nullptr || k <= 256);
+    warp_slots = warp_direct ? k : JW_SLOTS;
+    warp_smem = (JW_BLOCK / 32) * (warp_direct ? 1u : 2u) * warp_slots * (u32) sizeof(u32);
     HP_CUDA(cudaMemcpyAsync(map, part, sizeof(u32) * n, cudaMemcpyDeviceToDevice, c.stream));
     device_fill<u32>(c, dest_cache, n, NULL_PART);
     HP_CUDA(cudaMemsetAsync(gain_cache, 0, sizeof(s32) * n, c.stream));
@@ -1206,7 +1339,12 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     }
     {
         KernTimer kt(c, "k_lp_warp");
-        k_lp_warp<<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
+        if (warp_direct) {
+            k_lp_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, warp_smem, c.stream>>>(a, ratio_pct, warp_slots);
+        } else {
+            k_lp_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, warp_smem, c.stream>>>(a, ratio_pct, warp_slots);
+        }
+        note_launch();
     }
     {
         KernTimer kt(c, "k_lp_block");
@@ -1270,7 +1408,12 @@ void JetLevel::weak() {
         }
         {
             KernTimer kt1(c, "k_weak_warp");
-            k_rb_warp<false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+            if (warp_direct) {
+                k_rb_warp<false, true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, warp_smem, c.stream>>>(a, r, warp_slots);
+            } else {
+                k_rb_warp<false, false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, warp_smem, c.stream>>>(a, r, warp_slots);
+            }
+            note_launch();
         }
         {
             KernTimer kt1(c, "k_weak_block");
@@ -1328,7 +1471,12 @@ void JetLevel::strong() {
         }
         {
             KernTimer kt1(c, "k_strong_warp");
-            k_rb_warp<true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, 0, c.stream>>>(a, r); note_launch();
+            if (warp_direct) {
+                k_rb_warp<true, true><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, warp_smem, c.stream>>>(a, r, warp_slots);
+            } else {
+                k_rb_warp<true, false><<<c.grid((u64) n * 32, JW_BLOCK), JW_BLOCK, warp_smem, c.stream>>>(a, r, warp_slots);
+            }
+            note_launch();
         }
         {
             KernTimer kt1(c, "k_strong_block");
@@ -1407,12 +1555,8 @@ void JetLevel::perform() {
             k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
         }
         {
-            KernTimer kt1(c, "k_delta_warp");
-            k_delta_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-        }
-        {
-            KernTimer kt1(c, "k_delta_block");
-            k_delta_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+            KernTimer kt1(c, "k_delta_chunk");
+            k_delta_chunk<<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
         }
         k_unmark<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }

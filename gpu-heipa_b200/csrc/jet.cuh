@@ -63,7 +63,12 @@ struct JetLevel {
     u32 *moves = nullptr;
     u32 *heavy = nullptr;
     u32 *heavy2 = nullptr;
+    unsigned long long *items = nullptr;  // delta pass chunk items
+    u32 items_cap = 0;
     u32 blk_slots = 0;  // block-tier table size
+    bool warp_direct = false;  // warp tier: direct-indexed (else hashed) tables
+    u32 warp_slots = 0;        // warp tier: table slots per warp
+    u32 warp_smem = 0;         // warp tier: dynamic shared memory per block
     size_t gain_rec = SIZE_MAX;   // instrumentation record of the last gain pass
     size_t delta_rec = SIZE_MAX;  // instrumentation record of the last delta pass
 
