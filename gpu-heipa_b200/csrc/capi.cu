@@ -481,6 +481,26 @@ int hp_kernel_timing(hp_ctx *ctx, const char *name, uint64_t *launches, double *
     });
 }
 
+int hp_kernel_log(hp_ctx *ctx, uint64_t index, char *name, size_t name_len, double *ms, double *bytes) {
+    if (!ctx) return HP_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (index == 0) {
+            ctx->c.sync();
+            ctx->c.instr.resolve();
+        }
+        const auto &log = ctx->c.instr.log;
+        if (index >= log.size()) throw hp::HpError{HP_ERR_ARG, "kernel log index past the end"};
+        const auto &r = log[index];
+        if (name && name_len) {
+            const size_t k = std::min(name_len - 1, r.name.size());
+            std::memcpy(name, r.name.data(), k);
+            name[k] = 0;
+        }
+        if (ms) *ms = r.ms;
+        if (bytes) *bytes = r.bytes;
+    });
+}
+
 int hp_event_record(hp_ctx *ctx, int slot) {
     if (!ctx) return HP_ERR_ARG;
     return guarded(ctx, [&] { HP_CUDA(cudaEventRecord(ctx->c.event(slot), ctx->c.stream)); });

@@ -112,6 +112,7 @@ void Instr::resolve() {
         t->launches += 1;
         t->ms += ms;
         t->bytes += r.bytes;
+        if (log.size() < LOG_MAX) log.push_back(Logged{r.name, (double) ms, r.bytes});
         pool.push_back(r.a);
         pool.push_back(r.b);
     }
@@ -125,6 +126,7 @@ void Instr::clear() {
     }
     pending.clear();
     totals.clear();
+    log.clear();
 }
 
 void Instr::destroy() {

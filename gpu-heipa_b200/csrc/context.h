@@ -83,9 +83,16 @@ struct Instr {
         double ms = 0.0;
         double bytes = 0.0;
     };
+    struct Logged {
+        std::string name;
+        double ms;
+        double bytes;
+    };
+    static constexpr size_t LOG_MAX = 1u << 20;  // resolved records kept in launch order
     bool enabled = false;
     std::vector<Rec> pending;
     std::vector<Total> totals;
+    std::vector<Logged> log;
     std::vector<cudaEvent_t> pool;
     cudaEvent_t get_event();
     // begin() returns a record index (or SIZE_MAX when disabled) for end().

@@ -16,8 +16,6 @@ constexpr u32 JW_SLOTS = 1024;     // ... whose block table fits this per-warp c
 constexpr int JW_BLOCK = 128;      // 4 warps per block
 constexpr u32 JB_SLOTS = 16384;    // largest per-block table (128 KB)
 constexpr int JB_BLOCK = 512;
-constexpr u32 AB_T = 32;           // afterburner / delta: thread-level degree
-constexpr u32 AB_W = 2048;         // afterburner / delta: warp-level degree
 constexpr u32 EMPTY = NO_BLOCK_ID;
 constexpr u32 NOKEY = 0xFFFFFFFFu;
 // During perform, map[] holds the new label of every vertex and the MOVED
@@ -52,8 +50,11 @@ struct JArgs {
     u32 *moves;
     u32 *heavy;
     u32 *heavy2;
-    unsigned long long *items;  // delta pass work items: (vertex << 32) | chunk
+    unsigned long long *items;  // chunk work items (afterburner, delta): (vertex << 32) | chunk
     u32 items_cap;
+    unsigned long long inval_all_min;  // moved-row entries from which perform resets every cache
+    s32 *abacc;  // afterburner partial sums of multi-chunk rows (zero between uses)
+    u32 *abcnt;  // afterburner finished chunks of multi-chunk rows (zero between uses)
     DevStatus *st;
 };
 
@@ -506,33 +507,90 @@ __global__ void __launch_bounds__(BLOCK) k_lp_filter(JArgs a) {
 }
 
 // afterburner (:269-331 / ProMap :273-320): contribution of neighbour v.
-__device__ __forceinline__ s32 ab_term(const JArgs &a, u32 u, s32 ug, u32 ou, u32 nu, u32 v, s32 w) {
-    const s32 vg = a.gain1[v];
-    if (!(vg > ug || (vg == ug && v < u))) return 0;
-    const u32 nv = a.dest_part[v], ov = a.map[v];
-    if (!a.code) {
-        const s32 t = (s32) (nv == nu) - (s32) (nv == ou) + (s32) (ov == ou) - (s32) (ov == nu);
-        return wmul(w, t);
+
+// Neighbour-loop kernels (afterburner, delta): rows up to CHUNK_THREAD_MAX
+// entries are handled by one thread; longer rows are cut into chunks of
+// CHUNK entries, one warp each, so that hub rows spread over the whole GPU.
+constexpr u32 CHUNK_THREAD_MAX = 32;
+constexpr u32 CHUNK = 1024;
+
+__device__ __forceinline__ u32 chunks_of(u32 len) { return (len + CHUNK - 1) / CHUNK; }
+
+// Appends nch chunk items of row u (all lanes of the warp call this; lanes
+// with nch == 0 append nothing). One atomic per warp reserves the slots.
+__device__ __forceinline__ void warp_emit_chunks(const JArgs &a, u32 u, u32 nch) {
+    u32 incl = nch;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(FULL, incl, o);
+        if (lane_id() >= o) incl += y;
     }
-    const s32 before_u = wsub(D(a, ou, ov), D(a, nu, ov));
-    const s32 after_u = wsub(D(a, ou, nv), D(a, nu, nv));
-    return wmul(w, wsub(after_u, before_u));
+    const u32 wtot = __shfl_sync(FULL, incl, 31);
+    u32 wbase = 0;
+    if (lane_id() == 31 && wtot) wbase = atomicAdd(&a.st->cnt[ST_HEAVY], wtot);
+    wbase = __shfl_sync(FULL, wbase, 31);
+    const u32 first = wbase + incl - nch;
+    for (u32 c = 0; c < nch; ++c) {
+        if (first + c < a.items_cap) a.items[first + c] = ((unsigned long long) u << 32) | c;
+        else set_error(&a.st->err, DEV_ERR_RANGE);
+    }
 }
 
-// Tier of a row for the neighbour-loop kernels: 0 thread, 1 warp, 2 block.
-__device__ __forceinline__ int loop_tier(u32 len) { return len <= AB_T ? 0 : (len <= AB_W ? 1 : 2); }
+// Entries [from, to) of chunk item `it`.
+__device__ __forceinline__ void chunk_range(const JArgs &a, unsigned long long it, u32 &u, u32 &from, u32 &to,
+                                            u32 &nch) {
+    u = (u32) (it >> 32);
+    from = (u32) it * CHUNK;
+    const u32 len = __ldg(&a.g.rowlen[u]);
+    to = len - from < CHUNK ? len : from + CHUNK;
+    nch = chunks_of(len);
+}
 
-// Sum over u's row of the afterburner terms, strided over a group of
-// `nthreads` threads starting at `tid` (wrap-around s32 arithmetic).
-__device__ __forceinline__ s32 ab_partial(const JArgs &a, u32 u, u32 tid, u32 nthreads) {
-    const s32 ug = a.gain1[u];
-    const u32 ou = a.map[u], nu = a.dest_part[u];
-    const u64 beg = a.g.rowptr[u];
-    const u32 len = a.g.rowlen[u];
+// Sum of the afterburner terms over entries [from, to) of u's row, strided
+// over a group of threads (wrap-around s32 arithmetic). The gains, targets
+// and labels read here are not written by the afterburner kernels, so they
+// are gathered through the non-coherent path, four entries at a time.
+__device__ __forceinline__ s32 ab_range(const JArgs &a, u32 u, s32 ug, u32 ou, u32 nu, u32 from, u32 to, u32 tid,
+                                        u32 nthreads) {
+    const u64 beg = __ldg(&a.g.rowptr[u]);
     s32 change = 0;
-#pragma unroll 4
-    for (u32 t = tid; t < len; t += nthreads)
-        change = wadd(change, ab_term(a, u, ug, ou, nu, a.g.adj[beg + t], g_ew(a.g, beg + t)));
+    for (u32 t0 = from + tid; t0 < to; t0 += 4 * nthreads) {
+        u32 v[4], nv[4], ov[4];
+        s32 w[4], vg[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u32 t = t0 + j * nthreads;
+            v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
+            w[j] = t < to ? g_ew(a.g, beg + t) : 0;
+        }
+        // only neighbours that move first (higher gain, or equal gain and a
+        // lower id) contribute: their target and label are gathered after
+        // the gains, still four at a time
+        bool first[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) vg[j] = v[j] != SENTINEL ? __ldg(&a.gain1[v[j]]) : 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
+            if (first[j]) {
+                nv[j] = __ldg(&a.dest_part[v[j]]);
+                ov[j] = __ldg(&a.map[v[j]]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!first[j]) continue;
+            s32 t;
+            if (!a.code) {
+                t = wmul(w[j], (s32) (nv[j] == nu) - (s32) (nv[j] == ou) + (s32) (ov[j] == ou) - (s32) (ov[j] == nu));
+            } else {
+                const s32 before_u = wsub(D(a, ou, ov[j]), D(a, nu, ov[j]));
+                const s32 after_u = wsub(D(a, ou, nv[j]), D(a, nu, nv[j]));
+                t = wmul(w[j], wsub(after_u, before_u));
+            }
+            change = wadd(change, t);
+        }
+    }
     return change;
 }
 
@@ -543,63 +601,57 @@ __global__ void __launch_bounds__(BLOCK) k_ab_thread(JArgs a) {
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
         const u64 i = base + threadIdx.x;
         bool lock = false;
-        int tier = -1;
-        u32 u = 0;
+        u32 u = 0, nch = 0;
         if (i < total) {
             u = a.cand[i];
-            tier = loop_tier(a.g.rowlen[u]);
-            if (tier == 0 && wadd(a.gain1[u], ab_partial(a, u, 0, 1)) >= 0) {
-                a.lock[u] = 1;
-                lock = true;
+            const u32 len = __ldg(&a.g.rowlen[u]);
+            if (len <= CHUNK_THREAD_MAX) {
+                const s32 ug = __ldg(&a.gain1[u]);
+                const u32 ou = __ldg(&a.map[u]), nu = __ldg(&a.dest_part[u]);
+                if (wadd(ug, ab_range(a, u, ug, ou, nu, 0, len, 0, 1)) >= 0) {
+                    a.lock[u] = 1;
+                    lock = true;
+                }
+            } else {
+                nch = chunks_of(len);
             }
         }
-        const u32 s1 = warp_append(&a.st->cnt[ST_HEAVY], tier == 1);
-        if (tier == 1) a.heavy[s1] = u;
-        const u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], tier == 2);
-        if (tier == 2) a.heavy2[s2] = u;
+        warp_emit_chunks(a, u, nch);
         const u32 s3 = block_append(&a.st->cnt[ST_MOVES], lock, sm);
         if (lock) a.moves[s3] = u;
     }
 }
 
-__global__ void k_ab_warp(JArgs a) {
-    const u32 total = a.st->cnt[ST_HEAVY];
+// One warp per chunk item. A row of one chunk is decided by its warp; for a
+// row of several chunks each warp adds its partial sum to abacc[u] and the
+// last warp to finish (counted in abcnt[u], after a fence) decides and resets
+// both words, so nothing waits for another warp.
+__global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
+    u32 total = a.st->cnt[ST_HEAVY];
+    if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
-        const u32 u = a.heavy[i];
-        const s32 change = (s32) warp_sum<u32>((u32) ab_partial(a, u, lane_id(), 32));
-        if (lane_id() == 0 && wadd(a.gain1[u], change) >= 0) {
-            a.lock[u] = 1;
-            a.moves[atomicAdd(&a.st->cnt[ST_MOVES], 1u)] = u;
-        }
-    }
-}
-
-// Block-wide sum of a u32 (all threads call; result valid in every thread).
-__device__ __forceinline__ u32 block_sum_u32(u32 v, u32 *sm) {
-    v = warp_sum<u32>(v);
-    if (lane_id() == 0) sm[warp_in_block()] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        u32 r = 0;
-        for (u32 w = 0; w < (blockDim.x >> 5); ++w) r += sm[w];
-        sm[32] = r;
-    }
-    __syncthreads();
-    v = sm[32];
-    __syncthreads();
-    return v;
-}
-
-__global__ void __launch_bounds__(JB_BLOCK) k_ab_block(JArgs a) {
-    __shared__ u32 sm[33];
-    const u32 total = a.st->cnt[ST_HEAVY2];
-    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
-        const u32 u = a.heavy2[i];
-        const s32 change = (s32) block_sum_u32((u32) ab_partial(a, u, threadIdx.x, blockDim.x), sm);
-        if (threadIdx.x == 0 && wadd(a.gain1[u], change) >= 0) {
-            a.lock[u] = 1;
-            a.moves[atomicAdd(&a.st->cnt[ST_MOVES], 1u)] = u;
+        u32 u, from, to, nch;
+        chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
+        const s32 ug = __ldg(&a.gain1[u]);
+        const u32 ou = __ldg(&a.map[u]), nu = __ldg(&a.dest_part[u]);
+        const s32 change = (s32) warp_sum<u32>((u32) ab_range(a, u, ug, ou, nu, from, to, lane_id(), 32));
+        if (lane_id() == 0) {
+            bool decide = nch == 1;
+            s32 tot = change;
+            if (!decide) {
+                atomicAdd(&a.abacc[u], change);
+                __threadfence();
+                if (atomicAdd(&a.abcnt[u], 1u) == nch - 1) {
+                    tot = atomicExch(&a.abacc[u], 0);
+                    a.abcnt[u] = 0;
+                    decide = true;
+                }
+            }
+            if (decide && wadd(ug, tot) >= 0) {
+                a.lock[u] = 1;
+                a.moves[atomicAdd(&a.st->cnt[ST_MOVES], 1u)] = u;
+            }
         }
     }
 }
@@ -622,7 +674,8 @@ __global__ void k_unmark(JArgs a) {
 // are read through the non-coherent path; four entries per thread are loaded
 // (ids, then labels, then old labels of moved neighbours) before the cache
 // resets are stored, which keeps four dependent gathers in flight.
-__device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 nthreads) {
+__device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 nthreads,
+                                                 bool inval) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     const u32 x = __ldg(&a.map[u]);
     const bool um = (x & MOVED) != 0;
@@ -653,11 +706,28 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
                 acc += (xv[j] & MOVED) ? c : 2 * c;
             }
         }
+        if (inval) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (v[j] != SENTINEL) a.dest_cache[v[j]] = NULL_PART;
+            for (int j = 0; j < 4; ++j)
+                if (v[j] != SENTINEL) a.dest_cache[v[j]] = NULL_PART;
+        }
     }
     return acc;
+}
+
+// When the moved rows hold at least inval_all_min entries, nearly every cache
+// is invalidated anyway: the delta kernels then skip the scattered resets and
+// k_inval_all resets all caches with one sequential fill. Only enabled where a
+// recomputed gain equals the cached one for every vertex whose neighbourhood
+// did not change (a fixed filter ratio per level, or the mapping objective).
+__device__ __forceinline__ bool scattered_inval(const JArgs &a) {
+    return (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] < a.inval_all_min;
+}
+
+__global__ void k_inval_all(JArgs a) {
+    if (scattered_inval(a)) return;
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < a.g.n; u += gridDim.x * blockDim.x)
+        a.dest_cache[u] = NULL_PART;
 }
 
 // Adds a per-thread s64 to the status word with one atomic per block.
@@ -673,14 +743,9 @@ __device__ __forceinline__ void block_add_s64(long long v, long long *dst) {
     }
 }
 
-// Rows of moved vertices up to DELTA_THREAD_MAX entries are handled by one
-// thread; longer rows are cut into chunks of DELTA_CHUNK entries, one warp per
-// chunk, so that hub rows spread over the whole GPU instead of one block.
-constexpr u32 DELTA_THREAD_MAX = 32;
-constexpr u32 DELTA_CHUNK = 1024;
-
 __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
+    const bool inval = scattered_inval(a);
     const u64 stride = (u64) gridDim.x * blockDim.x;
     long long acc = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -688,44 +753,32 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
         u32 u = 0, nch = 0;
         if (i < total) {
             u = a.moves[i];
-            const u32 len = a.g.rowlen[u];
-            if (len <= DELTA_THREAD_MAX) acc += delta_range(a, u, 0, len, 0, 1);
-            else nch = (len + DELTA_CHUNK - 1) / DELTA_CHUNK;
+            const u32 len = __ldg(&a.g.rowlen[u]);
+            if (len <= CHUNK_THREAD_MAX) acc += delta_range(a, u, 0, len, 0, 1, inval);
+            else nch = chunks_of(len);
         }
-        // warp-aggregated reservation of the chunk items
-        u32 incl = nch;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const u32 y = __shfl_up_sync(FULL, incl, o);
-            if (lane_id() >= o) incl += y;
-        }
-        const u32 wtot = __shfl_sync(FULL, incl, 31);
-        u32 wbase = 0;
-        if (lane_id() == 31 && wtot) wbase = atomicAdd(&a.st->cnt[ST_HEAVY], wtot);
-        wbase = __shfl_sync(FULL, wbase, 31);
-        const u32 first = wbase + incl - nch;
-        for (u32 c = 0; c < nch; ++c) {
-            if (first + c < a.items_cap) a.items[first + c] = ((unsigned long long) u << 32) | c;
-            else set_error(&a.st->err, DEV_ERR_RANGE);
-        }
+        warp_emit_chunks(a, u, nch);
     }
     block_add_s64(acc, &a.st->sum[SUM_DELTA]);
 }
 
-__global__ void __launch_bounds__(BLOCK) k_delta_chunk(JArgs a) {
+// Six blocks per SM (at most 40 registers): the pass is bound by dependent
+// gathers, so resident warps matter more than registers. The objective delta
+// is added with one atomic per warp, so no warp waits for the others of its
+// block at the end.
+__global__ void __launch_bounds__(BLOCK, 6) k_delta_chunk(JArgs a) {
     u32 total = a.st->cnt[ST_HEAVY];
     if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    const bool inval = scattered_inval(a);
     long long acc = 0;
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
-        const unsigned long long it = a.items[i];
-        const u32 u = (u32) (it >> 32);
-        const u32 from = (u32) it * DELTA_CHUNK;
-        const u32 len = a.g.rowlen[u];
-        const u32 to = len - from < DELTA_CHUNK ? len : from + DELTA_CHUNK;
-        acc += delta_range(a, u, from, to, lane_id(), 32);
+        u32 u, from, to, nch;
+        chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
+        acc += delta_range(a, u, from, to, lane_id(), 32, inval);
     }
-    block_add_s64(acc, &a.st->sum[SUM_DELTA]);
+    acc = warp_sum<long long>(acc);
+    if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
 }
 
 constexpr u32 APPLY_SMEM_K = 4096;  // block weights accumulated in shared memory up to this k
@@ -1185,6 +1238,9 @@ JArgs make_args(JetLevel &L) {
     a.heavy2 = L.heavy2;
     a.items = L.items;
     a.items_cap = L.items_cap;
+    a.abacc = L.abacc;
+    a.inval_all_min = L.cache_pure ? (L.g.m + 1) / 2 : ~0ull;
+    a.abcnt = L.abcnt;
     a.st = L.ctx->d_status;
     a.blk_slots = L.blk_slots;
     return a;
@@ -1305,10 +1361,14 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     moves = c.balloc<u32>(n);
     heavy = c.balloc<u32>(n);
     heavy2 = c.balloc<u32>(n);
-    // chunk items of the delta pass: one per row of <= DELTA_CHUNK entries,
-    // so at most n + m / DELTA_CHUNK + 1
-    items_cap = (u32) std::min<u64>(0xFFFFFFFFull, (u64) n + g.m / DELTA_CHUNK + 1);
+    // chunk items (afterburner candidates, delta moves; each vertex at most
+    // once): one per row of <= CHUNK entries, so at most n + m / CHUNK + 1
+    items_cap = (u32) std::min<u64>(0xFFFFFFFFull, (u64) n + g.m / CHUNK + 1);
     items = c.balloc<unsigned long long>(items_cap);
+    abacc = c.balloc<s32>(n);
+    abcnt = c.balloc<u32>(n);
+    HP_CUDA(cudaMemsetAsync(abacc, 0, sizeof(s32) * n, c.stream));
+    HP_CUDA(cudaMemsetAsync(abcnt, 0, sizeof(u32) * n, c.stream));
     epoch = 0;
     blk_slots = block_slots_for(k);
     // warp tier: direct-indexed table of k values when k is small enough
@@ -1373,12 +1433,8 @@ void JetLevel::lp(u32 ratio_pct) {
         k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }
     {
-        KernTimer kt1(c, "k_ab_warp");
-        k_ab_warp<<<c.grid((u64) n * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    }
-    {
-        KernTimer kt1(c, "k_ab_block");
-        k_ab_block<<<c.sm_count * 4, JB_BLOCK, 0, c.stream>>>(a); note_launch();
+        KernTimer kt1(c, "k_ab_chunk");
+        k_ab_chunk<<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }
     HP_LAUNCH_CHECK();
 }
@@ -1558,6 +1614,7 @@ void JetLevel::perform() {
             KernTimer kt1(c, "k_delta_chunk");
             k_delta_chunk<<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
         }
+        k_inval_all<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
         k_unmark<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }
     HP_LAUNCH_CHECK();
@@ -1570,6 +1627,9 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
     JetLevel L;
     L.setup(ctx, g, k, lmax, D, part);
     const bool promap = D != nullptr;
+    // one filter ratio per level (or none for the mapping objective): a
+    // recomputed gain then equals a still-valid cached one
+    L.cache_pure = promap || !ultra;
     s64 best_obj = obj;
     s32 best_max = maxw;
     std::vector<u32> ratios;
@@ -1622,7 +1682,9 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
                 // entry of a moved row adj (+ ew), the neighbour's label and
                 // its cache reset
                 const double ent = (double) st.sum[SUM_PERF_ENTRIES];
-                ctx.instr.pending[L.delta_rec].bytes = 36.0 * nm + (g.ew ? 16.0 : 12.0) * ent;
+                const bool all = L.cache_pure && (u64) st.sum[SUM_PERF_ENTRIES] >= (g.m + 1) / 2;
+                ctx.instr.pending[L.delta_rec].bytes =
+                    36.0 * nm + (g.ew ? 16.0 : 12.0) * ent - (all ? 4.0 * ent - 4.0 * g.n : 0.0);
             }
             if (!promap) {
                 if (nm == 0) {

@@ -63,14 +63,19 @@ struct JetLevel {
     u32 *moves = nullptr;
     u32 *heavy = nullptr;
     u32 *heavy2 = nullptr;
-    unsigned long long *items = nullptr;  // delta pass chunk items
+    unsigned long long *items = nullptr;  // chunk work items (afterburner, delta)
     u32 items_cap = 0;
+    s32 *abacc = nullptr;  // afterburner partial sums of multi-chunk rows
+    u32 *abcnt = nullptr;  // afterburner finished-chunk counts of multi-chunk rows
     u32 blk_slots = 0;  // block-tier table size
     bool warp_direct = false;  // warp tier: direct-indexed (else hashed) tables
     u32 warp_slots = 0;        // warp tier: table slots per warp
     u32 warp_smem = 0;         // warp tier: dynamic shared memory per block
     size_t gain_rec = SIZE_MAX;   // instrumentation record of the last gain pass
     size_t delta_rec = SIZE_MAX;  // instrumentation record of the last delta pass
+    // true when every cached gain would be recomputed identically from an
+    // unchanged neighbourhood (then perform may reset all caches at once)
+    bool cache_pure = false;
 
     void setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle *d, const u32 *part);
     // Each of these fills `moves` and leaves the move count in the status

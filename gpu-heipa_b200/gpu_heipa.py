@@ -67,6 +67,7 @@ _SIG = {
     "hp_last_solve_stats": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "hp_instrument": (_int, [_vp, _int]),
     "hp_kernel_timing": (_int, [_vp, ctypes.c_char_p, _vp, _vp, _vp]),
+    "hp_kernel_log": (_int, [_vp, _u64, ctypes.c_char_p, ctypes.c_size_t, _vp, _vp]),
     "hp_event_record": (_int, [_vp, _int]),
     "hp_event_elapsed": (_int, [_vp, _int, _int, _vp]),
     "hp_kernel_launches": (_u64, []),
@@ -421,6 +422,16 @@ class Context:
 
     def instrument(self, enable=True):
         self._check(_L.hp_instrument(self.h, int(enable)))
+
+    def kernel_log(self):
+        """Per-launch kernel-timer records [(name, ms, bytes)] in launch order."""
+        out, i = [], 0
+        buf = ctypes.create_string_buffer(64)
+        ms, by = _dbl(), _dbl()
+        while _L.hp_kernel_log(self.h, i, buf, 64, ctypes.byref(ms), ctypes.byref(by)) == 0:
+            out.append((buf.value.decode(), ms.value, by.value))
+            i += 1
+        return out
 
     def kernel_timing(self, name):
         l, ms, b = _u64(), ctypes.c_double(), ctypes.c_double()

@@ -172,6 +172,11 @@ int hp_last_solve_stats(const hp_ctx *ctx, double *phase_ms5, int64_t *initial_o
  * hp_kernel_timing reports launches, total ms and algorithmic bytes. */
 int hp_instrument(hp_ctx *ctx, int enable);
 int hp_kernel_timing(hp_ctx *ctx, const char *name, uint64_t *launches, double *ms, double *bytes);
+/* Per-launch records of the kernel timers in launch order (at most 2^20 per
+ * enable): name, device milliseconds and algorithmic bytes of record `index`;
+ * index 0 first waits for the stream. Returns HP_ERR_ARG past the last record.
+ * A profiling aid without a counterpart in the reference. */
+int hp_kernel_log(hp_ctx *ctx, uint64_t index, char *name, size_t name_len, double *ms, double *bytes);
 
 /* Records event `slot` (0..7) on the context's stream; hp_event_elapsed
  * returns the milliseconds between two recorded slots (synchronises). */
