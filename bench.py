@@ -6,6 +6,11 @@ the seed, unit vertex weights, edge weights uniform in [1,10]; k = 64,
 imbalance 0.03, config default. One step = one full partition (coarsening,
 contraction, initial partitioning, Jet refinement) of that graph.
 
+Other workloads (--workload): grid256; the process-mapping configurations
+rgg23_hm / rgg23_hm_ultra / rgg23_im (3D RGG, 8,388,608 points, mean degree
+14, hierarchy 4:8:6, distance 1:10:100); rmat18 and rgg20_hm are small
+profiling cases.
+
 value: undirected input edges / device time per step, graph resident in HBM
   (CUDA events on the library's stream, max over ranks).
 e2e:   same metric through hp_partition with pinned host buffers: host->device
@@ -37,14 +42,28 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "gpu-heipa_b200"))
 
+RMAT_DESC = "R-MAT scale {s}, edge factor 16, (0.57,0.19,0.19,0.05), edge weights U[1,10], k=64, eps=0.03"
+RGG_DESC = ("3D RGG {n} points, mean degree 14, edge weights U[1,100], explicit unit vertex weights, "
+            "hierarchy 4:8:6, distance 1:10:100, eps=0.03, {mode}")
+# task "partition": GPU-HeiPa (config from --config); task "map": GPU-HeiProMap
+# with a fixed hierarchy and mode. "sample" is the bounded CPU-baseline input
+# (same generator and parameters, smaller size).
 WORKLOADS = {
-    "rmat22": dict(kind="rmat", scale=22, ef=16, k=64, desc="R-MAT scale 22, edge factor 16, (0.57,0.19,0.19,0.05), "
-                                                          "edge weights U[1,10], k=64, eps=0.03"),
-    "rmat18": dict(kind="rmat", scale=18, ef=16, k=64, desc="R-MAT scale 18, edge factor 16, (0.57,0.19,0.19,0.05), "
-                                                          "edge weights U[1,10], k=64, eps=0.03 (profiling case)"),
-    "grid256": dict(kind="grid", w=256, h=256, k=16, desc="2D grid 256x256, unit weights, k=16, eps=0.03"),
+    "rmat22": dict(kind="rmat", scale=22, task="partition", k=64, desc=RMAT_DESC.format(s=22),
+                   sample=dict(kind="rmat", scale=18)),
+    "rmat18": dict(kind="rmat", scale=18, task="partition", k=64, desc=RMAT_DESC.format(s=18) + " (profiling case)",
+                   sample=dict(kind="rmat", scale=18)),
+    "grid256": dict(kind="grid", w=256, h=256, task="partition", k=16,
+                    desc="2D grid 256x256, unit weights, k=16, eps=0.03", sample=dict(kind="grid", w=256, h=256)),
+    "rgg23_hm": dict(kind="rgg", n=8388608, task="map", mode="HM", hier=[4, 8, 6], dist=[1, 10, 100],
+                     desc=RGG_DESC.format(n=8388608, mode="HM"), sample=dict(kind="rgg", n=262144)),
+    "rgg23_hm_ultra": dict(kind="rgg", n=8388608, task="map", mode="HM-ultra", hier=[4, 8, 6], dist=[1, 10, 100],
+                           desc=RGG_DESC.format(n=8388608, mode="HM-ultra"), sample=dict(kind="rgg", n=262144)),
+    "rgg23_im": dict(kind="rgg", n=8388608, task="map", mode="IM", hier=[4, 8, 6], dist=[1, 10, 100],
+                     desc=RGG_DESC.format(n=8388608, mode="IM"), sample=dict(kind="rgg", n=262144)),
+    "rgg20_hm": dict(kind="rgg", n=1048576, task="map", mode="HM", hier=[4, 8, 6], dist=[1, 10, 100],
+                     desc=RGG_DESC.format(n=1048576, mode="HM") + " (profiling case)", sample=dict(kind="rgg", n=262144)),
 }
-CPU_SAMPLE_SCALE = 18
 # kernel timers with algorithmic byte counts; the roofline reports the one with
 # the largest device time in the timed region
 ROOFLINE_KERNELS = ("contract", "jet_gain", "k_delta")
@@ -55,10 +74,48 @@ KERNEL_TIMERS = ("contract", "jet_gain", "k_lp_dispatch", "k_lp_warp", "k_lp_blo
                  "k_strong_dispatch", "k_strong_warp", "k_strong_block")
 
 
-def make_graph(H, wl, seed):
-    if wl["kind"] == "rmat":
-        return H.Graph.rmat(wl["scale"], wl["ef"], 0.57, 0.19, 0.19, 1, 10, seed)
-    return H.Graph.grid(wl["w"], wl["h"])
+def make_graph(H, spec, seed):
+    if spec["kind"] == "rmat":
+        return H.Graph.rmat(spec["scale"], 16, 0.57, 0.19, 0.19, 1, 10, seed)
+    if spec["kind"] == "rgg":
+        return H.Graph.rgg3d(spec["n"], 14.0, 1, 100, seed, True)
+    return H.Graph.grid(spec["w"], spec["h"])
+
+
+def config_of(wl, args):
+    return args.config if wl["task"] == "partition" else wl["mode"]
+
+
+def solve_device(ctx, dg, wl, args, out):
+    """One step on a graph resident in HBM; returns the objective (cut or J)."""
+    if wl["task"] == "partition":
+        return ctx.partition_graph(dg, wl["k"], 0.03, args.config, args.seed, out=out)[1]
+    return ctx.process_map_graph(dg, wl["hier"], wl["dist"], 0.03, wl["mode"], args.seed, out=out)[1]
+
+
+def solve_host(ctx, hg, wl, args, out):
+    """One step through the host-buffer entry point (upload and download inside)."""
+    if wl["task"] == "partition":
+        return ctx.partition(hg, wl["k"], 0.03, args.config, args.seed, out=out)[1]
+    return ctx.process_map(hg, wl["hier"], wl["dist"], 0.03, wl["mode"], args.seed, out=out)[1]
+
+
+def oracle_solve(O, og, wl, args):
+    """The CPU oracle restatement of the same task (test infrastructure)."""
+    if wl["task"] == "partition":
+        return O.partition(og, wl["k"], 0.03, args.config == "ultra", args.seed)[1]
+    if wl["mode"] == "IM":
+        return O.map_im(og, wl["hier"], wl["dist"], 0.03, args.seed)[1]
+    return O.map_hm(og, wl["hier"], wl["dist"], 0.03, wl["mode"] == "HM-ultra", args.seed)[1]
+
+
+def sample_desc(wl):
+    sp = wl["sample"]
+    if sp["kind"] == "rmat":
+        return f"R-MAT scale {sp['scale']} (same generator parameters), same task"
+    if sp["kind"] == "rgg":
+        return f"3D RGG {sp['n']} points (same generator parameters), same task"
+    return wl["desc"]
 
 
 def measured_peaks():
@@ -157,15 +214,15 @@ def barrier(world):
         dist.barrier()
 
 
-def cpu_oracle_run(H, seed, scale, k):
+def cpu_oracle_run(H, wl, args):
+    """Times the oracle on the workload's bounded sample: (edges, seconds, objective)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    g = H.Graph.rmat(scale, 16, 0.57, 0.19, 0.19, 1, 10, seed)
+    g = make_graph(H, wl["sample"], args.seed)
     og = O.Graph(g.xadj, g.adj, g.ew, g.vw)
     t0 = time.perf_counter()
-    _, cut = O.partition(og, k, 0.03, False, seed)
-    dt = time.perf_counter() - t0
-    return g.m // 2, dt, cut
+    obj = oracle_solve(O, og, wl, args)
+    return g.m // 2, time.perf_counter() - t0, obj
 
 
 def run_reference(args, world, rank):
@@ -173,32 +230,21 @@ def run_reference(args, world, rank):
         return 0
     import gpu_heipa as H
     wl = WORKLOADS[args.workload]
-    scale = CPU_SAMPLE_SCALE if wl["kind"] == "rmat" else None
     times, edges = [], 0
     for i in range(args.warmup + args.steps):
-        if wl["kind"] == "rmat":
-            e, dt, _ = cpu_oracle_run(H, args.seed, scale, wl["k"])
-        else:
-            sys.path.insert(0, os.path.join(ROOT, "oracle"))
-            import oracle as O
-            g = make_graph(H, wl, args.seed)
-            og = O.Graph(g.xadj, g.adj, g.ew, g.vw)
-            t0 = time.perf_counter()
-            O.partition(og, wl["k"], 0.03, False, args.seed)
-            dt, e = time.perf_counter() - t0, g.m // 2
+        e, dt, _ = cpu_oracle_run(H, wl, args)
         if i >= args.warmup:
             times.append(dt)
             edges = e
     ms = 1000.0 * sum(times) / len(times)
     value = edges / (ms / 1000.0)
-    sample = (f"R-MAT scale {scale} (same generator parameters, k={wl['k']})" if scale else wl["desc"])
     line = {
         "metric": "partition_throughput", "value": value, "unit": "edges/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": wl["desc"], "parallelism": "cpu"},
+        "config": {"workload": wl["desc"], "config": config_of(wl, args), "parallelism": "cpu"},
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1, "kind": "port", "sample": sample_desc(wl)},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -208,14 +254,13 @@ def run_reference(args, world, rank):
 def run_ours(args, world, rank, local):
     import gpu_heipa as H
     wl = WORKLOADS[args.workload]
-    k = wl["k"]
     g = make_graph(H, wl, args.seed)
     edges = g.m // 2
     ctx = H.Context(local, H.arena_estimate(g.n, g.m, g.ew is not None, g.vw is not None))
     dg = ctx.upload(g)
     part = np.empty(g.n, np.uint32)
     for _ in range(args.warmup):
-        ctx.partition_graph(dg, k, 0.03, args.config, args.seed, out=part)
+        solve_device(ctx, dg, wl, args, part)
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -225,8 +270,7 @@ def run_ours(args, world, rank, local):
     ctx.event_record(0)
     cuts = []
     for _ in range(args.steps):
-        _, cut = ctx.partition_graph(dg, k, 0.03, args.config, args.seed, out=part)
-        cuts.append(cut)
+        cuts.append(solve_device(ctx, dg, wl, args, part))
     ctx.event_record(1)
     ms_total = ctx.event_elapsed(0, 1)
     launches = (H.kernel_launches() - l0) / args.steps
@@ -258,11 +302,11 @@ def run_ours(args, world, rank, local):
         hg, hpart = g, np.empty(g.n, np.uint32)
     e2e_steps = 0 if args.no_e2e else args.steps
     for _ in range(0 if args.no_e2e else max(1, args.warmup // 2)):
-        ctx.partition(hg, k, 0.03, args.config, args.seed, out=hpart)
+        solve_host(ctx, hg, wl, args, hpart)
     barrier(world)
     ctx.event_record(2)
     for _ in range(e2e_steps):
-        ctx.partition(hg, k, 0.03, args.config, args.seed, out=hpart)
+        solve_host(ctx, hg, wl, args, hpart)
     ctx.event_record(3)
     e2e_ms_total = ctx.event_elapsed(2, 3) if e2e_steps else 0.0
     barrier(world)
@@ -290,16 +334,16 @@ def run_ours(args, world, rank, local):
                                   "GB/s": (timing[x]["bytes"] / (timing[x]["ms"] / 1000.0) / 1e9)
                                   if timing[x]["ms"] else None} for x in timing}}
     cpu = None
-    if world == 1 and not args.no_cpu_baseline and wl["kind"] == "rmat":
-        e, dt, ccut = cpu_oracle_run(H, args.seed, CPU_SAMPLE_SCALE, k)
+    if world == 1 and not args.no_cpu_baseline:
+        e, dt, cobj = cpu_oracle_run(H, wl, args)
         cpu = {"value": e / dt, "unit": "edges/s", "cores": 1, "kind": "port",
-               "sample": f"one partition of R-MAT scale {CPU_SAMPLE_SCALE} (same generator parameters), k={k}, "
-                         f"{dt:.1f} s", "cut": ccut}
+               "sample": f"one solve of {sample_desc(wl)}, {dt:.1f} s", "objective": cobj}
     line = {
         "metric": "partition_throughput", "value": value, "unit": "edges/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": wl["desc"], "n": g.n, "undirected_edges": edges, "k": k, "config": args.config,
+        "config": {"workload": wl["desc"], "n": g.n, "undirected_edges": edges,
+                   "k": wl["k"] if wl["task"] == "partition" else int(np.prod(wl["hier"])), "config": config_of(wl, args),
                    "seed": args.seed, "parallelism": f"replicas{world}",
                    "l2": "input CSR (%.2f GB) larger than L2 (126 MB)" % (h2d / 1e9)},
         "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -308,7 +352,8 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
-        "quality": {"cut": cuts[-1], "phase_ms": stats["phase_ms"], "levels": stats["levels"],
+        "quality": {("cut" if wl["task"] == "partition" else "J"): cuts[-1], "phase_ms": stats["phase_ms"],
+                    "levels": stats["levels"],
                     "arena_peak_bytes": arena_peak},
     }
     print(json.dumps(line), flush=True)

@@ -78,9 +78,10 @@ def build(verbose=False, jobs=None):
         out = os.path.join(BIN, app)
         if not os.path.exists(src):
             continue
-        if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(src), lib_time, hdr_time):
+        app_hdr = _newest(glob.glob(os.path.join(HERE, "apps", "*.h")))
+        if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(src), lib_time, hdr_time, app_hdr):
             continue
-        _run(["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src, "-o", out,
+        _run(["g++", "-O2", "-std=c++17", "-Wall", "-I" + os.path.join(ROOT, "include"), src, "-o", out,
               "-L" + os.path.dirname(LIB), "-lgpuheipa", "-Wl,-rpath,$ORIGIN/../lib"])
     return LIB
 

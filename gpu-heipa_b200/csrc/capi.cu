@@ -453,6 +453,20 @@ int hp_last_solve_stats(const hp_ctx *ctx, double *ms5, int64_t *initial_obj, in
     return HP_OK;
 }
 
+int hp_last_solve_maxw(const hp_ctx *ctx, int32_t *initial_maxw, int32_t *final_maxw) {
+    if (!ctx) return HP_ERR_ARG;
+    if (initial_maxw) *initial_maxw = ctx->last.initial_maxw;
+    if (final_maxw) *final_maxw = ctx->last.final_maxw;
+    return HP_OK;
+}
+
+int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t *m) {
+    if (!ctx || index >= ctx->last.level_n.size()) return HP_ERR_ARG;
+    if (n) *n = ctx->last.level_n[index];
+    if (m) *m = ctx->last.level_m[index];
+    return HP_OK;
+}
+
 int hp_instrument(hp_ctx *ctx, int enable) {
     if (!ctx) return HP_ERR_ARG;
     return guarded(ctx, [&] {

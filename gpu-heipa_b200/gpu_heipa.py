@@ -65,6 +65,8 @@ _SIG = {
     "hp_map": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_map_graph": (_int, [_vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_last_solve_stats": (_int, [_vp, _vp, _vp, _vp, _vp]),
+    "hp_last_solve_maxw": (_int, [_vp, _vp, _vp]),
+    "hp_last_solve_level": (_int, [_vp, _u32, _vp, _vp]),
     "hp_instrument": (_int, [_vp, _int]),
     "hp_kernel_timing": (_int, [_vp, ctypes.c_char_p, _vp, _vp, _vp]),
     "hp_kernel_log": (_int, [_vp, _u64, ctypes.c_char_p, ctypes.c_size_t, _vp, _vp]),
@@ -374,18 +376,18 @@ class Context:
                                           _p(part), ctypes.byref(c)))
         return part, c.value
 
-    def process_map(self, g, hierarchy, distance, imbalance=0.03, config="HM", seed=0):
+    def process_map(self, g, hierarchy, distance, imbalance=0.03, config="HM", seed=0, out=None):
         """GPU-HeiProMap: returns (mapping, J) with J over directed entries."""
         hier, dist = _a_u32(hierarchy), _a_i32(distance)
-        part = np.empty(g.n, np.uint32)
+        part = np.empty(g.n, np.uint32) if out is None else out
         J = _i64()
         self._check(_L.hp_map(self.h, g.n, g.m, _p(g.xadj), _p(g.adj), _p(g.ew), _p(g.vw), _p(hier), _p(dist),
                               len(hier), float(imbalance), MAP_MODES[config], int(seed), _p(part), ctypes.byref(J)))
         return part, J.value
 
-    def process_map_graph(self, dg, hierarchy, distance, imbalance=0.03, config="HM", seed=0):
+    def process_map_graph(self, dg, hierarchy, distance, imbalance=0.03, config="HM", seed=0, out=None):
         hier, dist = _a_u32(hierarchy), _a_i32(distance)
-        part = np.empty(dg.n, np.uint32)
+        part = np.empty(dg.n, np.uint32) if out is None else out
         J = _i64()
         self._check(_L.hp_map_graph(self.h, dg.h, _p(hier), _p(dist), len(hier), float(imbalance), MAP_MODES[config],
                                     int(seed), _p(part), ctypes.byref(J)))
@@ -396,7 +398,13 @@ class Context:
         o, lm, lv = _i64(), _i32(), _u32()
         self._check(_L.hp_last_solve_stats(self.h, ms, ctypes.byref(o), ctypes.byref(lm), ctypes.byref(lv)))
         keys = ("coarsening", "contraction", "initial_partitioning", "uncontraction", "refinement")
-        return dict(phase_ms=dict(zip(keys, list(ms))), initial_obj=o.value, lmax=lm.value, levels=lv.value)
+        im, fm = _i32(), _i32()
+        self._check(_L.hp_last_solve_maxw(self.h, ctypes.byref(im), ctypes.byref(fm)))
+        sizes, ln, lmm = [], _u32(), _u64()
+        while _L.hp_last_solve_level(self.h, len(sizes), ctypes.byref(ln), ctypes.byref(lmm)) == 0:
+            sizes.append((ln.value, lmm.value))
+        return dict(phase_ms=dict(zip(keys, list(ms))), initial_obj=o.value, lmax=lm.value, levels=lv.value,
+                    initial_maxw=im.value, final_maxw=fm.value, level_sizes=sizes)
 
     def event_record(self, slot):
         self._check(_L.hp_event_record(self.h, int(slot)))

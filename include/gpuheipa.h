@@ -167,6 +167,12 @@ int hp_map_graph(hp_ctx *ctx, const hp_graph *g, const uint32_t *hier, const int
  * initial partitioning, uncontraction, refinement (solver.h:319-328 keys). */
 int hp_last_solve_stats(const hp_ctx *ctx, double *phase_ms5, int64_t *initial_obj, int32_t *lmax,
                         uint32_t *levels);
+/* Maximum block weight after initial partitioning and at the end of the last
+ * solve (the "Init./Final max block w" lines of solver.h:301-329). */
+int hp_last_solve_maxw(const hp_ctx *ctx, int32_t *initial_maxw, int32_t *final_maxw);
+/* Size of hierarchy level `index` of the last solve (level 0 = input), the
+ * per-level "n m" lines of solver.h:358; HP_ERR_ARG past the last level. */
+int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t *m);
 
 /* Enables CUDA-event timing of the contraction and Jet-gain kernels on ctx;
  * hp_kernel_timing reports launches, total ms and algorithmic bytes. */
