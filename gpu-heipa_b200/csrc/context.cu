@@ -26,10 +26,20 @@ void Arena::init(size_t bytes) {
     peak_ = 0;
 }
 
+void Arena::attach(void *p, size_t bytes) {
+    base_ = (char *) p;
+    size_ = bytes & ~(ALIGN - 1);
+    front_ = 0;
+    back_ = size_;
+    peak_ = 0;
+    owns_ = false;
+}
+
 void Arena::destroy() {
-    if (base_) cudaFree(base_);
+    if (base_ && owns_) cudaFree(base_);
     base_ = nullptr;
     size_ = front_ = back_ = peak_ = 0;
+    owns_ = true;
 }
 
 void *Arena::front(size_t bytes) {
@@ -76,7 +86,7 @@ cudaEvent_t Instr::get_event() {
 }
 
 size_t Instr::begin(cudaStream_t s, const char *name, double bytes) {
-    if (!enabled) return SIZE_MAX;
+    if (!enabled || capturing) return SIZE_MAX;
     Rec r;
     r.name = name;
     r.a = get_event();
@@ -151,13 +161,13 @@ static double now_ms() {
 }
 
 ProfScope::ProfScope(Ctx &ctx, const char *nm) : c(ctx), name(nm) {
-    if (!c.prof.enabled) return;
+    if (!c.prof.enabled || c.prof.capturing) return;
     cudaStreamSynchronize(c.stream);
     t0 = now_ms();
 }
 
 ProfScope::~ProfScope() {
-    if (!c.prof.enabled) return;
+    if (!c.prof.enabled || c.prof.capturing) return;
     cudaStreamSynchronize(c.stream);
     c.prof.add(name, now_ms() - t0);
 }
@@ -168,7 +178,23 @@ cudaEvent_t Ctx::event(int slot) {
     return events[slot];
 }
 
+Ctx &Ctx::worker(size_t i) {
+    while (workers.size() <= i) {
+        std::unique_ptr<Ctx> w(new Ctx());
+        try {
+            w->init(device, 0);
+        } catch (...) {
+            w->destroy();
+            throw;
+        }
+        workers.push_back(std::move(w));
+    }
+    return *workers[i];
+}
+
 void Ctx::destroy() {
+    for (auto &w: workers) w->destroy();
+    workers.clear();
     if (stream) cudaStreamSynchronize(stream);
     for (cudaEvent_t &e: events)
         if (e) {

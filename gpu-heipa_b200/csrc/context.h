@@ -9,6 +9,7 @@
 // alignment, and an error return instead of abort() on exhaustion.
 #pragma once
 #include <cuda_runtime.h>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -33,6 +34,8 @@ struct HpError {
 class Arena {
 public:
     void init(size_t bytes);
+    // Uses [p, p + bytes) of memory owned by someone else (never freed here).
+    void attach(void *p, size_t bytes);
     void destroy();
     void *front(size_t bytes);
     void *back(size_t bytes);
@@ -48,6 +51,7 @@ public:
 private:
     char *base_ = nullptr;
     size_t size_ = 0, front_ = 0, back_ = 0, peak_ = 0;
+    bool owns_ = true;
 };
 
 // Restores the back (scratch) end of the arena when leaving a scope.
@@ -90,6 +94,7 @@ struct Instr {
     };
     static constexpr size_t LOG_MAX = 1u << 20;  // resolved records kept in launch order
     bool enabled = false;
+    bool capturing = false;  // stream capture in progress: records are skipped
     std::vector<Rec> pending;
     std::vector<Total> totals;
     std::vector<Logged> log;
@@ -108,6 +113,7 @@ struct Instr {
 // default (no synchronisation is added to the normal path).
 struct PhaseProf {
     bool enabled = false;
+    bool capturing = false;  // stream capture in progress: scopes are skipped
     std::vector<std::pair<std::string, double> > totals;
     std::vector<std::pair<std::string, u64> > counts;
     void add(const char *name, double ms);
@@ -130,6 +136,11 @@ struct Ctx {
     PhaseProf prof;
     cudaEvent_t events[8] = {};
     cudaEvent_t event(int slot);  // created on first use
+    // Worker contexts (own stream and status word, no arena of their own)
+    // for running independent sub-solves concurrently; created on first use
+    // and kept until destroy().
+    std::vector<std::unique_ptr<Ctx> > workers;
+    Ctx &worker(size_t i);
 
     void init(int dev, size_t arena_bytes);
     void destroy();

@@ -45,7 +45,6 @@ struct JArgs {
     u32 *lock;
     u32 *dest_part;
     s32 *gain1;
-    u32 epoch;
     u32 *cand;
     u32 *moves;
     u32 *heavy;
@@ -1042,7 +1041,8 @@ __global__ void k_maxv(const s32 *bw, u32 k, s32 max_b_w, int *out) {
 }
 
 // B(x) for x = p * width, p in [0, k]: weight of candidates with key < x.
-__global__ void k_bounds(const u32 *skeys, const long long *prefix, u32 c, u32 k, u32 width, long long *B) {
+__global__ void k_bounds(const u32 *skeys, const long long *prefix, const u32 *d_c, u32 k, u32 width, long long *B) {
+    const u32 c = *d_c;
     for (u32 p = blockIdx.x * blockDim.x + threadIdx.x; p <= k; p += gridDim.x * blockDim.x) {
         const u64 x = (u64) p * width;
         u32 lo = 0, hi = c;
@@ -1055,7 +1055,9 @@ __global__ void k_bounds(const u32 *skeys, const long long *prefix, u32 c, u32 k
     }
 }
 
-__global__ void k_weak_filter(JArgs a, const u32 *svals, const long long *prefix, const long long *B, u32 c) {
+__global__ void k_weak_filter(JArgs a, const u32 *svals, const long long *prefix, const long long *B,
+                              const u32 *d_c) {
+    const u32 c = *d_c;
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < c; base += stride) {
         const u64 i = base + threadIdx.x;
@@ -1072,8 +1074,9 @@ __global__ void k_weak_filter(JArgs a, const u32 *svals, const long long *prefix
     }
 }
 
-__global__ void k_strong_filter(JArgs a, const u32 *svals, const long long *prefix, const long long *B, u32 c,
-                                long long *evict_adjust, long long *mpre) {
+__global__ void k_strong_filter(JArgs a, const u32 *svals, const long long *prefix, const long long *B,
+                                const u32 *d_c, long long *evict_adjust, long long *mpre) {
+    const u32 c = *d_c;
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < c; base += stride) {
         const u64 i = base + threadIdx.x;
@@ -1166,10 +1169,18 @@ __global__ void k_strong_assign(JArgs a, const long long *mpre, const long long 
     }
 }
 
+// dst[i] = src[i] for i < *d_count.
+__global__ void k_copy_count(u32 *dst, const u32 *src, const u32 *d_count) {
+    const u32 c = *d_count;
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) dst[i] = src[i];
+}
+
 // Fallback slots in ascending vertex order (one thread; at most one
 // straddling vertex per chunk boundary reaches this).
-__global__ void k_strong_fallback(JArgs a, const u32 *fail, u32 nf, const long long *es, long long *max_v) {
+__global__ void k_strong_fallback(JArgs a, const u32 *fail, const u32 *d_nf, const long long *es, long long *max_v) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const u32 nf = *d_nf;
+    if (nf == 0) return;
     long long mv = *max_v;
     for (u32 i = 0; i < nf; ++i) {
         const u32 u = fail[i];
@@ -1231,7 +1242,6 @@ JArgs make_args(JetLevel &L) {
     a.lock = L.lock;
     a.dest_part = L.dest_part;
     a.gain1 = L.gain1;
-    a.epoch = L.epoch;
     a.cand = L.cand;
     a.moves = L.moves;
     a.heavy = L.heavy;
@@ -1369,7 +1379,6 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     abcnt = c.balloc<u32>(n);
     HP_CUDA(cudaMemsetAsync(abacc, 0, sizeof(s32) * n, c.stream));
     HP_CUDA(cudaMemsetAsync(abcnt, 0, sizeof(u32) * n, c.stream));
-    epoch = 0;
     blk_slots = block_slots_for(k);
     // warp tier: direct-indexed table of k values when k is small enough
     // (for the mapping objective the candidate scoring loops over the table,
@@ -1490,17 +1499,20 @@ void JetLevel::weak() {
             }
         },
         &c.d_status->cnt[ST_CAND]);
-    const u32 cc = c.read_status().cnt[ST_CAND];
-    radix_sort_pairs<u32>(c, ck, cands, cc, 0, bits_for((u64) MAX_BUCKETS * k * sections + 1));
-    long long *prefix = c.balloc<long long>((u64) cc + 1);
+    // the candidate count stays on the device: the sort, the scan and the
+    // filter read it there (no host synchronisation inside the step)
+    const u32 *d_cc = &c.d_status->cnt[ST_CAND];
+    radix_sort_pairs<u32>(c, ck, cands, n, 0, bits_for((u64) MAX_BUCKETS * k * sections + 1), d_cc);
+    long long *prefix = c.balloc<long long>((u64) n + 1);
     const DGraph gg = g;
     device_scan<long long>(
-        c, (u64) cc + 1, [=] __device__(u64 i) -> long long { return i < cc ? (long long) g_vw(gg, cands[i]) : 0; },
-        [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr);
+        c, (u64) n + 1,
+        [=] __device__(u64 i) -> long long { return i < *d_cc ? (long long) g_vw(gg, cands[i]) : 0; },
+        [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr, d_cc, 1);
     long long *B = c.balloc<long long>((u64) k + 1);
-    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B); note_launch();
+    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, d_cc, k, width, B); note_launch();
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_MOVES], 0, sizeof(u32), c.stream));
-    k_weak_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc); note_launch();
+    k_weak_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, d_cc); note_launch();
     HP_LAUNCH_CHECK();
 }
 
@@ -1552,34 +1564,36 @@ void JetLevel::strong() {
             }
         },
         &c.d_status->cnt[ST_CAND]);
-    const u32 cc = c.read_status().cnt[ST_CAND];
-    radix_sort_pairs<u32>(c, ck, cands, cc, 0, bits_for((u64) MAX_BUCKETS * k * sections + 2));
-    long long *prefix = c.balloc<long long>((u64) cc + 1);
+    const u32 *d_cc = &c.d_status->cnt[ST_CAND];
+    radix_sort_pairs<u32>(c, ck, cands, n, 0, bits_for((u64) MAX_BUCKETS * k * sections + 2), d_cc);
+    long long *prefix = c.balloc<long long>((u64) n + 1);
     const DGraph gg = g;
     device_scan<long long>(
-        c, (u64) cc + 1, [=] __device__(u64 i) -> long long { return i < cc ? (long long) g_vw(gg, cands[i]) : 0; },
-        [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr);
+        c, (u64) n + 1,
+        [=] __device__(u64 i) -> long long { return i < *d_cc ? (long long) g_vw(gg, cands[i]) : 0; },
+        [=] __device__(u64 i, long long p, long long) { prefix[i] = p; }, (long long *) nullptr, d_cc, 1);
     long long *B = c.balloc<long long>((u64) k + 1);
-    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, cc, k, width, B); note_launch();
+    k_bounds<<<c.grid(k + 1, BLOCK), BLOCK, 0, c.stream>>>(ck, prefix, d_cc, k, width, B); note_launch();
     long long *ea = c.balloc<long long>(k);
     long long *es = c.balloc<long long>((u64) k + 1);
-    long long *mpre = c.balloc<long long>((u64) cc + 1);
+    long long *mpre = c.balloc<long long>((u64) n + 1);
     HP_CUDA(cudaMemsetAsync(ea, 0, sizeof(long long) * k, c.stream));
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_MOVES], 0, sizeof(u32), c.stream));
-    k_strong_filter<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, cc, ea, mpre); note_launch();
+    k_strong_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, cands, prefix, B, d_cc, ea, mpre); note_launch();
     long long *max_v = (long long *) &c.d_status->sum[3];
     k_cookie<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, B, ea, es, max_v); note_launch();
     u32 *fail = c.balloc<u32>(n);
     u32 *n_fail = &c.d_status->cnt[ST_HEAVY];
     HP_CUDA(cudaMemsetAsync(n_fail, 0, sizeof(u32), c.stream));
-    k_strong_assign<<<c.grid(cc, BLOCK), BLOCK, 0, c.stream>>>(a, mpre, ea, es, fail, n_fail); note_launch();
+    k_strong_assign<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, mpre, ea, es, fail, n_fail); note_launch();
     HP_LAUNCH_CHECK();
-    const u32 nf = c.read_status().cnt[ST_HEAVY];
-    if (nf) {
-        u32 *fk = c.balloc<u32>(nf);
-        HP_CUDA(cudaMemcpyAsync(fk, fail, sizeof(u32) * nf, cudaMemcpyDeviceToDevice, c.stream));
-        radix_sort_pairs<u32>(c, fk, fail, nf, 0, 32);
-        k_strong_fallback<<<1, 32, 0, c.stream>>>(a, fail, nf, es, max_v); note_launch();
+    {
+        // fallback slots in ascending vertex id; the failure count stays on
+        // the device (usually zero: every kernel then returns at once)
+        u32 *fk = c.balloc<u32>(n);
+        k_copy_count<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(fk, fail, n_fail); note_launch();
+        radix_sort_pairs<u32>(c, fk, fail, n, 0, bits_for(n), n_fail);
+        k_strong_fallback<<<1, 32, 0, c.stream>>>(a, fail, n_fail, es, max_v); note_launch();
         HP_LAUNCH_CHECK();
     }
 }
@@ -1587,7 +1601,6 @@ void JetLevel::strong() {
 void JetLevel::perform() {
     Ctx &c = *ctx;
     ProfScope prof(c, "jet.perform");
-    ++epoch;
     JArgs a = make_args(*this);
     const u32 n = g.n;
     HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
@@ -1620,6 +1633,54 @@ void JetLevel::perform() {
     HP_LAUNCH_CHECK();
 }
 
+void JetLevel::release_graphs() {
+    for (StepGraph &sg: step_graphs) cudaGraphExecDestroy(sg.exec);
+    step_graphs.clear();
+}
+
+void JetLevel::run_step(int kind, u32 ratio_pct) {
+    Ctx &c = *ctx;
+    auto body = [&] {
+        if (kind == 0) lp(ratio_pct);
+        else if (kind == 1) weak();
+        else strong();
+        perform();
+        HP_CUDA(cudaMemcpyAsync(c.h_status, c.d_status, sizeof(DevStatus), cudaMemcpyDeviceToHost, c.stream));
+    };
+    if (!graphs) {
+        body();
+        c.sync();
+        return;
+    }
+    cudaGraphExec_t exec = nullptr;
+    for (const StepGraph &sg: step_graphs)
+        if (sg.kind == kind && sg.ratio == ratio_pct) exec = sg.exec;
+    if (!exec) {
+        // Scratch allocated inside the step is released when it returns and
+        // nothing else allocates while the level's iterations run, so the
+        // addresses baked into the graph stay valid for every replay.
+        cudaGraph_t graph = nullptr;
+        HP_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        c.instr.capturing = c.prof.capturing = true;
+        try {
+            body();
+        } catch (...) {
+            c.instr.capturing = c.prof.capturing = false;
+            cudaStreamEndCapture(c.stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        c.instr.capturing = c.prof.capturing = false;
+        HP_CUDA(cudaStreamEndCapture(c.stream, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        HP_CUDA(e);
+        step_graphs.push_back(StepGraph{kind, ratio_pct, exec});
+    }
+    HP_CUDA(cudaGraphLaunch(exec, c.stream));
+    c.sync();
+}
+
 void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultra, u32 level, s64 &obj, s32 &maxw,
                 const DistOracle *D) {
     if (g.n == 0 || k <= 1) return;
@@ -1630,6 +1691,7 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
     // one filter ratio per level (or none for the mapping objective): a
     // recomputed gain then equals a still-valid cached one
     L.cache_pure = promap || !ultra;
+    L.graphs = g.m <= JET_GRAPH_MAX_M && !ctx.prof.enabled;
     s64 best_obj = obj;
     s32 best_max = maxw;
     std::vector<u32> ratios;
@@ -1640,30 +1702,29 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
         while (iteration < JET_MAX_ITERATIONS) {
             iteration += 1;
             bool lp_iter = false;
+            int step = 0;
             if (!promap) {
                 if (maxw <= lmax) {
-                    L.lp(ratio);
+                    step = 0;
                     lp_iter = true;
                     balance_iteration = 0;
                 } else if (balance_iteration < JET_MAX_WEAK_ITERATIONS) {
-                    L.weak();
+                    step = 1;
                 } else {
-                    L.strong();
+                    step = 2;
                 }
             } else {
                 if (maxw <= lmax) {
-                    L.lp(ratio);
+                    step = 0;
                     lp_iter = true;
                     balance_iteration = 0;
                 } else {
                     balance_iteration++;
-                    if (balance_iteration < JET_MAX_WEAK_ITERATIONS) L.weak();
-                    else L.strong();
+                    step = balance_iteration < JET_MAX_WEAK_ITERATIONS ? 1 : 2;
                 }
             }
-            L.perform();
-            ProfScope prof_status(ctx, "jet.status");
-            const DevStatus &st = ctx.read_status();
+            L.run_step(step, ratio);
+            const DevStatus &st = *ctx.h_status;
             if (st.err) throw HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
             const u32 nm = st.cnt[ST_MOVES];
             if (lp_iter && L.gain_rec < ctx.instr.pending.size()) {

@@ -58,7 +58,6 @@ struct JetLevel {
     u32 *lock = nullptr;
     u32 *dest_part = nullptr;
     s32 *gain1 = nullptr;
-    u32 epoch = 0;
     u32 *cand = nullptr;
     u32 *moves = nullptr;
     u32 *heavy = nullptr;
@@ -89,7 +88,32 @@ struct JetLevel {
     // Single pass helpers used by tests: recompute gains for all vertices
     // whose cache is invalid (the "Jet-gain" kernel).
     void gain_pass(u32 ratio_pct);
+
+    // One Jet iteration: the step (0 = lp with ratio_pct, 1 = weak, 2 =
+    // strong), perform, and the status word copied to the host; returns after
+    // the stream is idle. With `graphs`, the sequence is captured into a CUDA
+    // graph on first use (per step kind and ratio) and replayed afterwards,
+    // so an iteration costs one graph launch and one host synchronisation.
+    bool graphs = false;
+    void run_step(int kind, u32 ratio_pct);
+    void release_graphs();
+    JetLevel() = default;
+    JetLevel(const JetLevel &) = delete;
+    JetLevel &operator=(const JetLevel &) = delete;
+    ~JetLevel() { release_graphs(); }
+
+private:
+    struct StepGraph {
+        int kind;
+        u32 ratio;
+        cudaGraphExec_t exec;
+    };
+    std::vector<StepGraph> step_graphs;
 };
+
+// Levels up to this many CSR entries replay their Jet iterations as CUDA
+// graphs (launch and synchronisation cost dominates there).
+constexpr u64 JET_GRAPH_MAX_M = 1ull << 24;
 
 // Status word slots used by Jet.
 constexpr int ST_MOVES = 3;

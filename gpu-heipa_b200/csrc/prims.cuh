@@ -38,9 +38,19 @@ __device__ __forceinline__ T block_exclusive_scan(T v, T &total, T *smem) {
 constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = BLOCK * SCAN_ITEMS;
 
+// Element count of a launch sized for n_max elements: min(n_max, *dn + add)
+// when a device count is given (read by the kernel, so the launch needs no
+// host synchronisation and can be captured in a CUDA graph).
+__device__ __forceinline__ u64 count_of(u64 n_max, const u32 *dn, u32 add) {
+    if (!dn) return n_max;
+    const u64 c = (u64) *dn + add;
+    return c < n_max ? c : n_max;
+}
+
 template<typename T, typename Load>
-__global__ void __launch_bounds__(BLOCK) k_scan_reduce(u64 n, Load load, T *tile_sums) {
+__global__ void __launch_bounds__(BLOCK) k_scan_reduce(u64 n, const u32 *dn, u32 dn_add, Load load, T *tile_sums) {
     __shared__ T sm[32];
+    n = count_of(n, dn, dn_add);
     const u64 base = (u64) blockIdx.x * SCAN_TILE;
     T s = T(0);
 #pragma unroll 4
@@ -69,8 +79,11 @@ __global__ void __launch_bounds__(1024) k_scan_tiles(T *sums, u32 ntiles, T *tot
 }
 
 template<typename T, typename Load, typename Store>
-__global__ void __launch_bounds__(BLOCK) k_scan_apply(u64 n, Load load, Store store, const T *tile_offsets) {
+__global__ void __launch_bounds__(BLOCK) k_scan_apply(u64 n, const u32 *dn, u32 dn_add, Load load, Store store,
+                                                      const T *tile_offsets) {
     __shared__ T sm[32];
+    n = count_of(n, dn, dn_add);
+    if ((u64) blockIdx.x * SCAN_TILE >= n) return;
     const u64 base = (u64) blockIdx.x * SCAN_TILE + (u64) threadIdx.x * SCAN_ITEMS;
     T vals[SCAN_ITEMS];
     T s = T(0);
@@ -92,16 +105,17 @@ __global__ void __launch_bounds__(BLOCK) k_scan_apply(u64 n, Load load, Store st
 
 // Exclusive scan over i in [0, n): prefix(i) = sum_{j<i} load(j); calls
 // store(i, prefix(i), load(i)) for every i. Writes the total to *total_dev
-// when given (device pointer). Deterministic for integer T.
+// when given (device pointer). With dn, n is min(n, *dn + dn_add), read on
+// the device. Deterministic for integer T.
 template<typename T, typename Load, typename Store>
-void device_scan(Ctx &ctx, u64 n, Load load, Store store, T *total_dev) {
+void device_scan(Ctx &ctx, u64 n, Load load, Store store, T *total_dev, const u32 *dn = nullptr, u32 dn_add = 0) {
     ScratchScope ss(ctx.arena);
     u64 nt = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (nt == 0) nt = 1;
     T *sums = ctx.balloc<T>(nt);
-    k_scan_reduce<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, load, sums); note_launch();
+    k_scan_reduce<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, dn, dn_add, load, sums); note_launch();
     k_scan_tiles<T><<<1, 1024, 0, ctx.stream>>>(sums, (u32) nt, total_dev); note_launch();
-    k_scan_apply<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, load, store, sums); note_launch();
+    k_scan_apply<T><<<(u32) nt, BLOCK, 0, ctx.stream>>>(n, dn, dn_add, load, store, sums); note_launch();
     HP_LAUNCH_CHECK();
 }
 
@@ -122,8 +136,10 @@ constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = BLOCK * RS_ITEMS;
 
 template<typename K>
-__global__ void __launch_bounds__(BLOCK) k_rs_hist(const K *keys, u64 n, int shift, u32 *hist, u32 ntiles) {
+__global__ void __launch_bounds__(BLOCK) k_rs_hist(const K *keys, u64 n, const u32 *dn, int shift, u32 *hist,
+                                                   u32 ntiles) {
     __shared__ u32 cnt[256];
+    n = count_of(n, dn, 0);
     cnt[threadIdx.x] = 0;
     __syncthreads();
     const u64 base = (u64) blockIdx.x * RS_TILE;
@@ -137,7 +153,9 @@ __global__ void __launch_bounds__(BLOCK) k_rs_hist(const K *keys, u64 n, int shi
 
 template<typename K>
 __global__ void __launch_bounds__(BLOCK) k_rs_scatter(const K *kin, const u32 *vin, K *kout, u32 *vout, u64 n,
-                                                       int shift, const u32 *offs, u32 ntiles) {
+                                                       const u32 *dn, int shift, const u32 *offs, u32 ntiles) {
+    n = count_of(n, dn, 0);
+    if ((u64) blockIdx.x * RS_TILE >= n) return;
     __shared__ u32 run[256];
     __shared__ u32 wc[BLOCK / 32][256];
     const int t = threadIdx.x, w = warp_in_block(), lane = lane_id();
@@ -174,8 +192,10 @@ __global__ void __launch_bounds__(BLOCK) k_rs_scatter(const K *kin, const u32 *v
 
 // Sorts n pairs by key bits [begin_bit, end_bit), stably; keys/vals are
 // updated in place (scratch double buffers come from the arena's back end).
+// With dn, the pair count is min(n, *dn), read on the device (buffers are
+// sized for n).
 template<typename K>
-void radix_sort_pairs(Ctx &ctx, K *keys, u32 *vals, u64 n, int begin_bit, int end_bit) {
+void radix_sort_pairs(Ctx &ctx, K *keys, u32 *vals, u64 n, int begin_bit, int end_bit, const u32 *dn = nullptr) {
     if (n <= 1 || end_bit <= begin_bit) return;
     ScratchScope ss(ctx.arena);
     u32 ntiles = (u32) ((n + RS_TILE - 1) / RS_TILE);
@@ -185,12 +205,12 @@ void radix_sort_pairs(Ctx &ctx, K *keys, u32 *vals, u64 n, int begin_bit, int en
     K *ks = keys, *kd = k_alt;
     u32 *vs = vals, *vd = v_alt;
     for (int shift = begin_bit; shift < end_bit; shift += 8) {
-        k_rs_hist<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, n, shift, hist, ntiles); note_launch();
+        k_rs_hist<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, n, dn, shift, hist, ntiles); note_launch();
         u64 hn = (u64) 256 * ntiles;
         device_scan<u32>(
             ctx, hn, [=] __device__(u64 i) -> u32 { return hist[i]; },
             [=] __device__(u64 i, u32 p, u32) { hist[i] = p; }, (u32 *) nullptr);
-        k_rs_scatter<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, vs, kd, vd, n, shift, hist, ntiles); note_launch();
+        k_rs_scatter<K><<<ntiles, BLOCK, 0, ctx.stream>>>(ks, vs, kd, vd, n, dn, shift, hist, ntiles); note_launch();
         HP_LAUNCH_CHECK();
         std::swap(ks, kd);
         std::swap(vs, vd);

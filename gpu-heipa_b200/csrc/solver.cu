@@ -1,8 +1,13 @@
 #include "solver.cuh"
 #include "prims.cuh"
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
+#include <exception>
+#include <mutex>
+#include <thread>
 
 #include "../host/initial_partition.h"
 
@@ -160,46 +165,143 @@ s64 solve_partition(Ctx &ctx, const DGraph &g, u32 k, double eps, bool ultra, u6
 
 namespace {
 
-// recursive_multisection_device (hierarchical_multisection.h:56-235)
-void hm_recurse(Ctx &ctx, const DGraph &g, const u32 *n_to_o, const std::vector<u32> &hier, u32 level,
-                std::vector<u32> &identifier, const std::vector<u32> &index_vec, const std::vector<u32> &k_rem,
-                double eps, s64 global_w, u32 global_k, u64 seed, bool ultra, u32 *global_part, SolveStats *stats) {
-    const u32 l = (u32) hier.size();
-    const u32 k_here = hier[level];
-    const u64 depth = identifier.size();
-    const double imb = adaptive_imbalance(eps, global_w, global_k, g.total_vw, k_rem[l - 1 - depth], l - depth);
-    const size_t mark = ctx.arena.front_mark();
-    u32 *tmp = ctx.falloc<u32>(g.n);
-    SolveStats sub;
-    solve_partition(ctx, g, k_here, imb, ultra, seed, tmp, stats ? &sub : nullptr);
-    if (stats) stats->add(sub);
-    if (depth == l - 1) {
-        u32 offset = 0;
-        for (u32 i = 0; i + 1 < l; ++i) offset += identifier[i] * index_vec[index_vec.size() - 1 - i];
-        k_scatter_leaf<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(tmp, n_to_o, g.n, offset, global_part); note_launch();
-        HP_LAUNCH_CHECK();
-        ctx.sync();
-        ctx.arena.front_release(mark);
+// One sub-solve of the hierarchical multisection: a subgraph (in the main
+// arena), its map to input vertex ids, the path of block ids that leads to it,
+// and its partition.
+struct HmTask {
+    DGraph g;
+    const u32 *n_to_o = nullptr;
+    std::vector<u32> identifier;
+    u32 *part = nullptr;
+};
+
+// Arena bytes a worker needs for one sub-solve of g (hierarchy, Jet scratch
+// and sorting buffers; the subgraph itself lives in the main arena).
+size_t worker_bytes(const DGraph &g) { return 96 * (size_t) g.m + 256 * (size_t) g.n + (64ull << 20); }
+
+constexpr size_t HM_MAX_WORKERS = 16;
+
+// Runs fn(ctx_w, task) for every task. The sub-solves are independent and
+// deterministic, so they run concurrently on worker contexts (one host
+// thread, stream and status word each, arena slices carved from the main
+// arena's free space); with room for one slice only, they run in order on the
+// main context. Results do not depend on the number of workers.
+template<typename Fn>
+void run_hm_tasks(Ctx &ctx, std::vector<HmTask> &tasks, Fn fn) {
+    size_t slice = 0;
+    for (const HmTask &t: tasks) slice = std::max(slice, worker_bytes(t.g));
+    slice = (slice + 4095) & ~(size_t) 4095;
+    const size_t free_bytes = ctx.arena.back_mark() - ctx.arena.front_mark();
+    size_t W = std::min<size_t>(tasks.size(), HM_MAX_WORKERS);
+    if (slice) W = std::min<size_t>(W, free_bytes / slice);
+    if (W <= 1) {
+        for (HmTask &t: tasks) fn(ctx, t);
         return;
     }
-    for (u32 id = 0; id < k_here; ++id) {
-        const size_t m2 = ctx.arena.front_mark();
-        u32 *sub_n_to_o_local = ctx.falloc<u32>(g.n);
-        u32 sub_n = 0;
-        DGraph sg = graph_induced(ctx, g, tmp, id, sub_n_to_o_local, sub_n);
-        if (sub_n == 0) {
-            ctx.arena.front_release(m2);
-            continue;
-        }
-        u32 *sub_n_to_o = ctx.falloc<u32>(sub_n);
-        k_compose<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(n_to_o, sub_n_to_o_local, sub_n, sub_n_to_o); note_launch();
-        HP_LAUNCH_CHECK();
-        identifier.push_back(id);
-        hm_recurse(ctx, sg, sub_n_to_o, hier, level - 1, identifier, index_vec, k_rem, eps, global_w, global_k, seed,
-                   ultra, global_part, stats);
-        identifier.pop_back();
-        ctx.arena.front_release(m2);
+    ScratchScope ss(ctx.arena);
+    char *slab = ctx.balloc<char>(W * slice);
+    ctx.sync();  // subgraphs and partition arrays are ready before workers start
+    std::vector<Ctx *> wc(W);
+    for (size_t w = 0; w < W; ++w) {
+        wc[w] = &ctx.worker(w);
+        wc[w]->arena.attach(slab + w * slice, slice);
     }
+    std::atomic<size_t> next{0};
+    std::vector<std::exception_ptr> errors(W);
+    std::vector<std::thread> threads;
+    for (size_t w = 0; w < W; ++w) {
+        threads.emplace_back([&, w] {
+            try {
+                HP_CUDA(cudaSetDevice(ctx.device));
+                for (size_t i = next++; i < tasks.size(); i = next++) {
+                    fn(*wc[w], tasks[i]);
+                    wc[w]->sync();
+                }
+            } catch (...) {
+                errors[w] = std::current_exception();
+                next = tasks.size();
+            }
+        });
+    }
+    for (std::thread &t: threads) t.join();
+    for (size_t w = 0; w < W; ++w) wc[w]->arena.destroy();
+    for (std::exception_ptr &e: errors)
+        if (e) std::rethrow_exception(e);
+}
+
+// recursive_multisection_device (hierarchical_multisection.h:56-235), level
+// by level: every subgraph of one hierarchy level is partitioned into the
+// level's number of parts, then the next level's subgraphs are induced from
+// those parts. Leaves write their parts, offset by the block-id path, into
+// global_part.
+void hm_solve(Ctx &ctx, const DGraph &g, const std::vector<u32> &hier, double eps, u64 seed, bool ultra,
+              u32 *global_part, SolveStats *stats) {
+    const u32 l = (u32) hier.size();
+    std::vector<u32> index_vec = {1};
+    for (u32 i = 0; i + 1 < l; ++i) index_vec.push_back(index_vec[i] * hier[i]);
+    std::vector<u32> k_rem(l);
+    u32 kp = 1;
+    for (u32 i = 0; i < l; ++i) {
+        k_rem[i] = kp * hier[i];
+        kp *= hier[i];
+    }
+    const u32 global_k = kp;
+    const s64 global_w = g.total_vw;
+    const size_t mark = ctx.arena.front_mark();
+    u32 *n_to_o = ctx.falloc<u32>(g.n);
+    device_iota(ctx, n_to_o, g.n);
+    std::vector<HmTask> cur(1);
+    cur[0].g = g;
+    cur[0].n_to_o = n_to_o;
+    std::mutex stats_mu;
+    for (u32 depth = 0; depth < l && !cur.empty(); ++depth) {
+        const u32 level = l - 1 - depth;
+        const u32 k_here = hier[level];
+        const bool leaf = depth == l - 1;
+        for (HmTask &t: cur) t.part = ctx.falloc<u32>(t.g.n);
+        run_hm_tasks(ctx, cur, [&](Ctx &wc, HmTask &t) {
+            const double imb = adaptive_imbalance(eps, global_w, global_k, t.g.total_vw, k_rem[l - 1 - depth], l - depth);
+            SolveStats sub;
+            solve_partition(wc, t.g, k_here, imb, ultra, seed, t.part, stats ? &sub : nullptr);
+            if (leaf) {
+                u32 offset = 0;
+                for (u32 i = 0; i + 1 < l; ++i) offset += t.identifier[i] * index_vec[index_vec.size() - 1 - i];
+                k_scatter_leaf<<<wc.grid(t.g.n, BLOCK), BLOCK, 0, wc.stream>>>(t.part, t.n_to_o, t.g.n, offset,
+                                                                              global_part); note_launch();
+                HP_LAUNCH_CHECK();
+                wc.sync();
+            }
+            if (stats) {
+                std::lock_guard<std::mutex> lock(stats_mu);
+                stats->add(sub);
+            }
+        });
+        if (leaf) break;
+        std::vector<HmTask> next;
+        for (HmTask &t: cur) {
+            for (u32 id = 0; id < k_here; ++id) {
+                const size_t m2 = ctx.arena.front_mark();
+                u32 *local = ctx.falloc<u32>(t.g.n);
+                u32 sub_n = 0;
+                DGraph sg = graph_induced(ctx, t.g, t.part, id, local, sub_n);
+                if (sub_n == 0) {
+                    ctx.arena.front_release(m2);
+                    continue;
+                }
+                u32 *sub_n_to_o = ctx.falloc<u32>(sub_n);
+                k_compose<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(t.n_to_o, local, sub_n, sub_n_to_o); note_launch();
+                HP_LAUNCH_CHECK();
+                HmTask c;
+                c.g = sg;
+                c.n_to_o = sub_n_to_o;
+                c.identifier = t.identifier;
+                c.identifier.push_back(id);
+                next.push_back(std::move(c));
+            }
+        }
+        cur = std::move(next);
+    }
+    ctx.sync();
     ctx.arena.front_release(mark);
 }
 
@@ -242,19 +344,7 @@ s64 solve_mapping(Ctx &ctx, const DGraph &g, const std::vector<u32> &hier, const
         }
     } else {
         // hierarchical_multisection (hierarchical_multisection.h:237-307)
-        std::vector<u32> index_vec = {1};
-        for (u32 i = 0; i + 1 < l; ++i) index_vec.push_back(index_vec[i] * hier[i]);
-        std::vector<u32> k_rem(l);
-        u32 p = 1;
-        for (u32 i = 0; i < l; ++i) {
-            k_rem[i] = p * hier[i];
-            p *= hier[i];
-        }
-        u32 *n_to_o = ctx.falloc<u32>(g.n);
-        device_iota(ctx, n_to_o, g.n);
-        std::vector<u32> identifier;
-        hm_recurse(ctx, g, n_to_o, hier, l - 1, identifier, index_vec, k_rem, eps, g.total_vw, k, seed, mode == 2,
-                   part, stats);
+        hm_solve(ctx, g, hier, eps, seed, mode == 2, part, stats);
         J = comm_cost_dev(ctx, g, part, D);
         if (stats) {
             s32 *bw = ctx.falloc<s32>(k);
