@@ -3,10 +3,14 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <new>
 
 #include "../host/generators.h"
 #include "../host/metis_io.h"
+#include "service.cuh"
 #include "solver.cuh"
 
 struct hp_ctx {
@@ -29,6 +33,13 @@ struct hp_jet {
 
 struct hp_host_graph {
     hp::HostCSR g;
+};
+
+struct hp_server {
+    hp::Ctx c;  // owns the request buffer (its arena) and the worker contexts
+    std::unique_ptr<hp::Service> svc;
+    std::mutex mu;
+    std::string last_error;
 };
 
 namespace {
@@ -435,6 +446,154 @@ int hp_map(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint
         }
         ctx->c.arena.front_release(fm);
     });
+}
+
+namespace {
+
+// Device bytes one request may use (input graph, hierarchy, Jet scratch);
+// rounded up by the service.
+size_t request_bytes(uint32_t n, uint64_t m, const int32_t *ew, const int32_t *vw) {
+    return hp::request_estimate(n, m, ew != nullptr, vw != nullptr);
+}
+
+std::function<hp::s64(hp::Ctx &)> partition_job(uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                                                 const int32_t *ew, const int32_t *vw, uint32_t k, double imbalance,
+                                                 int ultra, uint64_t seed, uint32_t *part) {
+    return [=](hp::Ctx &c) -> hp::s64 {
+        hp::DGraph g = hp::graph_upload(c, n, m, xadj, adj, ew, vw);
+        hp::u32 *d = c.falloc<hp::u32>(n);
+        const hp::s64 cut = hp::solve_partition(c, g, k, imbalance, ultra != 0, seed, d, nullptr);
+        HP_CUDA(cudaMemcpyAsync(part, d, sizeof(hp::u32) * n, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        return cut;
+    };
+}
+
+std::function<hp::s64(hp::Ctx &)> mapping_job(uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                                               const int32_t *ew, const int32_t *vw, std::vector<hp::u32> hier,
+                                               std::vector<hp::s32> dist, double imbalance, int mode, uint64_t seed,
+                                               uint32_t *part) {
+    return [=](hp::Ctx &c) -> hp::s64 {
+        hp::DGraph g = hp::graph_upload(c, n, m, xadj, adj, ew, vw);
+        hp::u32 *d = c.falloc<hp::u32>(n);
+        const hp::s64 J = hp::solve_mapping(c, g, hier, dist, imbalance, mode, seed, d, nullptr);
+        HP_CUDA(cudaMemcpyAsync(part, d, sizeof(hp::u32) * n, cudaMemcpyDeviceToHost, c.stream));
+        c.sync();
+        return J;
+    };
+}
+
+}  // namespace
+
+int hp_partition_batch(hp_ctx *ctx, hp_batch_item *items, uint32_t count, uint32_t workers) {
+    if (!ctx || (count && !items)) return HP_ERR_ARG;
+    for (uint32_t i = 0; i < count; ++i)
+        if (!items[i].part || items[i].k == 0) return HP_ERR_ARG;
+    int first_error = HP_OK;
+    const int rc = guarded(ctx, [&] {
+        hp::ScratchScope ss(ctx->c.arena);
+        const size_t free_bytes = ctx->c.arena.back_mark() - ctx->c.arena.front_mark();
+        char *base = ctx->c.balloc<char>(free_bytes);
+        std::vector<hp::u64> ids(count);
+        {
+            hp::Service svc(ctx->c, base, free_bytes, workers ? workers : 8);
+            for (uint32_t i = 0; i < count; ++i) {
+                hp_batch_item &it = items[i];
+                auto job = std::make_shared<hp::Job>();
+                job->bytes = request_bytes(it.n, it.m, it.ew, it.vw);
+                job->run = partition_job(it.n, it.m, it.xadj, it.adj, it.ew, it.vw, it.k, it.imbalance, it.ultra,
+                                         it.seed, it.part);
+                ids[i] = svc.submit(job);
+            }
+            for (uint32_t i = 0; i < count; ++i) {
+                std::shared_ptr<hp::Job> j = svc.wait(ids[i]);
+                items[i].status = j->status;
+                items[i].cut = j->objective;
+                if (j->status != HP_OK && first_error == HP_OK) {
+                    first_error = j->status;
+                    ctx->c.last_error = "batch item " + std::to_string(i) + ": " + j->error;
+                }
+            }
+        }
+    });
+    if (rc != HP_OK) return rc;
+    return first_error;
+}
+
+int hp_server_create(int device, size_t buffer_bytes, uint32_t workers, hp_server **out) {
+    if (!out || buffer_bytes == 0) return HP_ERR_ARG;
+    *out = nullptr;
+    hp_server *s = new (std::nothrow) hp_server();
+    if (!s) return HP_ERR_OOM;
+    int rc = guarded_host([&] {
+        s->c.init(device, buffer_bytes);
+        s->svc.reset(new hp::Service(s->c, s->c.arena.base(), s->c.arena.capacity(), workers ? workers : 8));
+    });
+    if (rc != HP_OK) {
+        s->svc.reset();
+        s->c.destroy();
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return HP_OK;
+}
+
+int hp_server_destroy(hp_server *s) {
+    if (!s) return HP_ERR_ARG;
+    s->svc.reset();  // finishes every queued request, then stops the workers
+    s->c.destroy();
+    delete s;
+    return HP_OK;
+}
+
+const char *hp_server_last_error(hp_server *s) { return s ? s->last_error.c_str() : "null server"; }
+
+int hp_server_submit_partition(hp_server *s, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                               const int32_t *ew, const int32_t *vw, uint32_t k, double imbalance, int ultra,
+                               uint64_t seed, uint32_t *part, uint64_t *request) {
+    if (!s || !xadj || (m && !adj) || !part || !request || k == 0) return HP_ERR_ARG;
+    return guarded_host([&] {
+        auto job = std::make_shared<hp::Job>();
+        job->bytes = request_bytes(n, m, ew, vw);
+        job->run = partition_job(n, m, xadj, adj, ew, vw, k, imbalance, ultra, seed, part);
+        *request = s->svc->submit(job);
+    });
+}
+
+int hp_server_submit_map(hp_server *s, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                         const int32_t *ew, const int32_t *vw, const uint32_t *hier, const int32_t *dist,
+                         uint32_t levels, double imbalance, int mode, uint64_t seed, uint32_t *part,
+                         uint64_t *request) {
+    if (!s || !xadj || (m && !adj) || !part || !request || mode < 0 || mode > 2) return HP_ERR_ARG;
+    return guarded_host([&] {
+        check_hier(hier, dist, levels);
+        auto job = std::make_shared<hp::Job>();
+        job->bytes = request_bytes(n, m, ew, vw);
+        job->run = mapping_job(n, m, xadj, adj, ew, vw, vec_u32(hier, levels), vec_s32(dist, levels), imbalance, mode,
+                               seed, part);
+        *request = s->svc->submit(job);
+    });
+}
+
+int hp_server_poll(hp_server *s, uint64_t request, int *done) {
+    if (!s || !done) return HP_ERR_ARG;
+    *done = s->svc->is_done(request) ? 1 : 0;
+    return HP_OK;
+}
+
+int hp_server_wait(hp_server *s, uint64_t request, int64_t *objective, double *latency_ms, double *run_ms) {
+    if (!s) return HP_ERR_ARG;
+    std::shared_ptr<hp::Job> j = s->svc->wait(request);
+    if (!j) return HP_ERR_ARG;
+    if (objective) *objective = j->objective;
+    if (latency_ms) *latency_ms = j->t_end - j->t_submit;
+    if (run_ms) *run_ms = j->t_end - j->t_start;
+    if (j->status != HP_OK) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->last_error = j->error;
+    }
+    return j->status;
 }
 
 int hp_last_solve_stats(const hp_ctx *ctx, double *ms5, int64_t *initial_obj, int32_t *lmax, uint32_t *levels) {

@@ -107,6 +107,14 @@ s32 lmax_of(s64 total_weight, u32 k, double eps) {
     return (s32) std::ceil((1.0 + eps) * ((double) total_weight / (double) k));
 }
 
+size_t request_estimate(u32 n, u64 m, bool has_ew, bool has_vw) {
+    // the terms of arena_estimate with the per-vertex and scratch shares of
+    // the hierarchy rounded up and a small fixed reserve instead of 512 MiB,
+    // so that small requests of a served stream reserve little memory
+    const double in = 4.0 * ((double) n + 1) * 2 + 4.0 * (double) m * (has_ew ? 2 : 1) + (has_vw ? 4.0 * n : 0.0);
+    return (size_t) (in + 96.0 * (double) m + 256.0 * (double) n + 16.0 * 1024 * 1024);
+}
+
 size_t arena_estimate(u32 n, u64 m, bool has_ew, bool has_vw) {
     // input graph + hierarchy (every padded level holds up to the fine level's
     // m entries of 8 bytes; power-law graphs keep ~90% of their edges for the

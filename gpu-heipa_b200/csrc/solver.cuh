@@ -44,5 +44,7 @@ s64 solve_mapping(Ctx &ctx, const DGraph &g, const std::vector<u32> &hier, const
 // Bytes of device arena a solve of a graph with n vertices and m directed
 // entries needs (hierarchy plus scratch), with a safety margin.
 size_t arena_estimate(u32 n, u64 m, bool has_ew, bool has_vw);
+// Device bytes one request of a batch or a served stream reserves.
+size_t request_estimate(u32 n, u64 m, bool has_ew, bool has_vw);
 
 } // namespace hp

@@ -75,6 +75,15 @@ _SIG = {
     "hp_kernel_launches": (_u64, []),
     "hp_profile": (_int, [_vp, _int]),
     "hp_profile_entry": (_int, [_vp, _u32, ctypes.c_char_p, ctypes.c_size_t, _vp, _vp]),
+    "hp_partition_batch": (_int, [_vp, _vp, _u32, _u32]),
+    "hp_server_create": (_int, [_int, ctypes.c_size_t, _u32, _vp]),
+    "hp_server_submit_partition": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
+    "hp_server_submit_map": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp,
+                                    _vp]),
+    "hp_server_poll": (_int, [_vp, _u64, _vp]),
+    "hp_server_wait": (_int, [_vp, _u64, _vp, _vp, _vp]),
+    "hp_server_last_error": (ctypes.c_char_p, [_vp]),
+    "hp_server_destroy": (_int, [_vp]),
     "hp_read_metis": (_int, [ctypes.c_char_p, _vp]),
     "hp_gen_grid": (_int, [_u32, _u32, _i32, _i32, _u64, _vp]),
     "hp_gen_rmat": (_int, [_u32, _u32, _dbl, _dbl, _dbl, _i32, _i32, _u64, _int, _vp]),
@@ -174,6 +183,72 @@ class Graph:
         _host_check(_L.hp_gen_rgg3d(n, mean_degree, w_lo, w_hi, seed, int(explicit_vw), ctypes.byref(g)),
                     "rgg generator failed")
         return Graph._from_handle(g)
+
+
+class BatchItem(ctypes.Structure):
+    """Mirror of hp_batch_item (include/gpuheipa.h)."""
+    _fields_ = [("n", ctypes.c_uint32), ("m", ctypes.c_uint64), ("xadj", _vp), ("adj", _vp), ("ew", _vp),
+                ("vw", _vp), ("k", ctypes.c_uint32), ("imbalance", ctypes.c_double), ("ultra", ctypes.c_int),
+                ("seed", ctypes.c_uint64), ("part", _vp), ("cut", ctypes.c_int64), ("status", ctypes.c_int)]
+
+
+class Server:
+    """Serving loop (hp_server_*): submit partitioning / mapping requests as
+    they arrive; each runs as soon as a worker and device memory are free.
+    The host arrays of a request are kept alive here until it is waited on."""
+
+    def __init__(self, device=0, buffer_bytes=8 << 30, workers=8):
+        self.h = _vp()
+        rc = _L.hp_server_create(device, buffer_bytes, workers, ctypes.byref(self.h))
+        if rc != 0:
+            self.h = None
+            raise HeiPaError(rc, "server creation failed")
+        self._keep = {}
+
+    def submit_partition(self, g, k, imbalance=0.03, config="default", seed=0):
+        part = np.empty(g.n, np.uint32)
+        rid = _u64()
+        _host_check(_L.hp_server_submit_partition(self.h, g.n, g.m, _p(g.xadj), _p(g.adj), _p(g.ew), _p(g.vw), int(k),
+                                                  float(imbalance), int(config == "ultra"), int(seed), _p(part),
+                                                  ctypes.byref(rid)), "submit failed")
+        self._keep[rid.value] = (g, part)
+        return rid.value
+
+    def submit_map(self, g, hierarchy, distance, imbalance=0.03, config="HM", seed=0):
+        hier, dist = _a_u32(hierarchy), _a_i32(distance)
+        part = np.empty(g.n, np.uint32)
+        rid = _u64()
+        _host_check(_L.hp_server_submit_map(self.h, g.n, g.m, _p(g.xadj), _p(g.adj), _p(g.ew), _p(g.vw), _p(hier),
+                                            _p(dist), len(hier), float(imbalance), MAP_MODES[config], int(seed),
+                                            _p(part), ctypes.byref(rid)), "submit failed")
+        self._keep[rid.value] = (g, part, hier, dist)
+        return rid.value
+
+    def done(self, rid):
+        d = _int()
+        _L.hp_server_poll(self.h, rid, ctypes.byref(d))
+        return bool(d.value)
+
+    def wait(self, rid):
+        """Returns (part, objective, latency_ms, run_ms)."""
+        obj, lat, run = _i64(), _dbl(), _dbl()
+        rc = _L.hp_server_wait(self.h, rid, ctypes.byref(obj), ctypes.byref(lat), ctypes.byref(run))
+        keep = self._keep.pop(rid, None)
+        if rc != 0:
+            raise HeiPaError(rc, _L.hp_server_last_error(self.h).decode())
+        return keep[1], obj.value, lat.value, run.value
+
+    def close(self):
+        if self.h:
+            _L.hp_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def kernel_launches():
@@ -392,6 +467,18 @@ class Context:
         self._check(_L.hp_map_graph(self.h, dg.h, _p(hier), _p(dist), len(hier), float(imbalance), MAP_MODES[config],
                                     int(seed), _p(part), ctypes.byref(J)))
         return part, J.value
+
+    def partition_batch(self, graphs, ks, imbalance=0.03, config="default", seed=0, workers=8):
+        """hp_partition_batch: [(part, cut)] for graphs[i] with ks[i] blocks."""
+        items = (BatchItem * len(graphs))()
+        parts = []
+        for i, (g, k) in enumerate(zip(graphs, ks)):
+            part = np.empty(g.n, np.uint32)
+            parts.append(part)
+            items[i] = BatchItem(g.n, g.m, _p(g.xadj), _p(g.adj), _p(g.ew), _p(g.vw), int(k), float(imbalance),
+                                 int(config == "ultra"), int(seed), _p(part), 0, 0)
+        self._check(_L.hp_partition_batch(self.h, items, len(graphs), workers))
+        return [(parts[i], items[i].cut) for i in range(len(graphs))]
 
     def last_solve_stats(self):
         ms = (ctypes.c_double * 5)()

@@ -196,6 +196,61 @@ uint64_t hp_kernel_launches(void);
 int hp_profile(hp_ctx *ctx, int enable);
 int hp_profile_entry(const hp_ctx *ctx, uint32_t index, char *name, size_t name_len, double *ms, uint64_t *count);
 
+/* ---- batched and served requests --------------------------------------------- */
+
+/* One graph of a batch (host buffers, caller-owned). The results part (n
+ * labels), cut and status are written by hp_partition_batch. */
+typedef struct hp_batch_item {
+    uint32_t n;
+    uint64_t m;
+    const uint32_t *xadj;
+    const uint32_t *adj;
+    const int32_t *ew; /* NULL: unit edge weights */
+    const int32_t *vw; /* NULL: unit vertex weights */
+    uint32_t k;
+    double imbalance;
+    int ultra;
+    uint64_t seed;
+    uint32_t *part; /* out */
+    int64_t cut;    /* out */
+    int status;     /* out: HP_OK or this item's error */
+} hp_batch_item;
+
+/* Partitions `count` independent graphs (GPU-HeiPa each, the same result as
+ * hp_partition on that graph alone). Up to `workers` graphs (0: 8) run at
+ * once on their own streams, each admitted by a device-memory estimate of its
+ * solve (input + 96 B per entry + 256 B per vertex + 16 MiB) into the
+ * context's free arena. Returns HP_OK, or the first failing item's status
+ * (hp_last_error names the item). No counterpart in the reference, which
+ * solves one graph per process. */
+int hp_partition_batch(hp_ctx *ctx, hp_batch_item *items, uint32_t count, uint32_t workers);
+
+/* Serving loop: requests are queued on submit and run as soon as a worker
+ * (0: 8) and enough of the server's device buffer (buffer_bytes, allocated at
+ * create) are free, oldest first, with smaller requests allowed past a
+ * blocked one a bounded number of times. Each request's result equals the
+ * plain call's (hp_partition / hp_map) on the same input. Host buffers passed
+ * to a submit must stay valid until its hp_server_wait returns. Safe to call
+ * from several host threads. No counterpart in the reference. */
+typedef struct hp_server hp_server;
+int hp_server_create(int device, size_t buffer_bytes, uint32_t workers, hp_server **out);
+int hp_server_submit_partition(hp_server *s, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                               const int32_t *ew, const int32_t *vw, uint32_t k, double imbalance, int ultra,
+                               uint64_t seed, uint32_t *part, uint64_t *request);
+int hp_server_submit_map(hp_server *s, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj,
+                         const int32_t *ew, const int32_t *vw, const uint32_t *hier, const int32_t *dist,
+                         uint32_t levels, double imbalance, int mode, uint64_t seed, uint32_t *part,
+                         uint64_t *request);
+/* done = 1 when the request has finished (or is unknown). */
+int hp_server_poll(hp_server *s, uint64_t request, int *done);
+/* Blocks until the request finishes; returns its status and writes its
+ * objective (cut or J), latency (submit to finish) and run time in ms. */
+int hp_server_wait(hp_server *s, uint64_t request, int64_t *objective, double *latency_ms, double *run_ms);
+/* Message of the last failed request returned by hp_server_wait. */
+const char *hp_server_last_error(hp_server *s);
+/* Finishes every queued request, then frees the server. */
+int hp_server_destroy(hp_server *s);
+
 /* ---- host utilities (no device work) --------------------------------------- */
 
 /* Replaces from_file (src/datastructures/host_graph.h:154-247). */
