@@ -61,6 +61,14 @@ WORKLOADS = {
                            desc=RGG_DESC.format(n=8388608, mode="HM-ultra"), sample=dict(kind="rgg", n=262144)),
     "rgg23_im": dict(kind="rgg", n=8388608, task="map", mode="IM", hier=[4, 8, 6], dist=[1, 10, 100],
                      desc=RGG_DESC.format(n=8388608, mode="IM"), sample=dict(kind="rgg", n=262144)),
+    "batch": dict(kind="mix", task="batch", count=512, nmin=1000, nmax=200000,
+                  desc="batch of 512 graphs, vertices log-uniform in [1000, 200000], generator uniform over "
+                       "{grid aspect U[1,4], R-MAT ef 8, RGG mean degree 10}, edge weights U[1,10], "
+                       "k power of two in 2..256, eps=0.03, default", sample=None),
+    "served": dict(kind="mix", task="served", count=300, rate=200.0, emin=10000, emax=2000000,
+                   desc="served: 300 Poisson requests at 200/s, undirected edges log-uniform in [1e4, 2e6], "
+                        "70% partition (k power of two 2..512) / 30% mapping (4:8:6 1:10:100, 2:4:8 1:5:50, "
+                        "8:16 1:20, HM), same generators, 8 workers", sample=None),
     "rgg20_hm": dict(kind="rgg", n=1048576, task="map", mode="HM", hier=[4, 8, 6], dist=[1, 10, 100],
                      desc=RGG_DESC.format(n=1048576, mode="HM") + " (profiling case)", sample=dict(kind="rgg", n=262144)),
 }
@@ -251,6 +259,155 @@ def run_reference(args, world, rank):
     return 0
 
 
+MAP_CHOICES = [([4, 8, 6], [1, 10, 100]), ([2, 4, 8], [1, 5, 50]), ([8, 16], [1, 20])]
+
+
+def mixed_graph(H, rng, n_target, seed, weights=(1, 10)):
+    """One graph of the batched / served mixes: grid (aspect U[1,4]), R-MAT
+    (edge factor 8, vertices rounded to a power of two) or RGG (mean degree
+    10), edge weights U[w_lo, w_hi]."""
+    kind = int(rng.integers(0, 3))
+    if kind == 0:
+        aspect = float(rng.uniform(1.0, 4.0))
+        w = max(2, int(round((n_target * aspect) ** 0.5)))
+        h = max(2, n_target // w)
+        return H.Graph.grid(w, h, weights[0], weights[1], seed)
+    if kind == 1:
+        scale = max(4, int(round(np.log2(n_target))))
+        return H.Graph.rmat(scale, 8, 0.57, 0.19, 0.19, weights[0], weights[1], seed)
+    return H.Graph.rgg3d(n_target, 10.0, weights[0], weights[1], seed, True)
+
+
+def run_batch(args, world, rank, local):
+    """Batched path: every graph of the mix through hp_partition_batch, against
+    one plain hp_partition per graph on the same GPU (both with host buffers)."""
+    import gpu_heipa as H
+    wl = WORKLOADS[args.workload]
+    rng = np.random.default_rng(args.seed + 1000 * rank)
+    graphs, ks = [], []
+    for i in range(wl["count"]):
+        n_t = int(np.exp(rng.uniform(np.log(wl["nmin"]), np.log(wl["nmax"]))))
+        graphs.append(mixed_graph(H, rng, n_t, args.seed + i))
+        ks.append(int(2 ** rng.integers(1, 9)))
+    edges = sum(g.m // 2 for g in graphs)
+    big = max(graphs, key=lambda g: g.m)
+    ctx = H.Context(local, 24 << 30)
+    for _ in range(args.warmup):
+        ctx.partition_batch(graphs[:64], ks[:64], 0.03, "default", args.seed, workers=args.workers)
+    barrier(world)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = ctx.partition_batch(graphs, ks, 0.03, "default", args.seed, workers=args.workers)
+        times.append(time.perf_counter() - t0)
+    # sequential plain runs of the same graphs (one step)
+    t0 = time.perf_counter()
+    plain_cuts = [ctx.partition(g, k, 0.03, "default", args.seed)[1] for g, k in zip(graphs, ks)]
+    plain_s = time.perf_counter() - t0
+    same = all(c == pc for (_, c), pc in zip(out, plain_cuts))
+    ctx.close()
+    s = reduce_max([sum(times) / len(times)], world)[0]
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "partition_throughput", "value": world * edges / s, "unit": "edges/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * s, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": wl["desc"], "graphs": len(graphs), "undirected_edges": edges,
+                   "largest_edges": big.m // 2, "workers": args.workers, "parallelism": f"replicas{world}",
+                   "timing": "host wall clock around hp_partition_batch (host buffers, uploads and downloads "
+                             "inside)"},
+        "e2e": {"value": world * edges / s, "unit": "edges/s", "graphs_per_s": world * len(graphs) / s,
+                "h2d_bytes_per_step": int(sum(4 * (g.n + 1) + 8 * g.m for g in graphs)),
+                "d2h_bytes_per_step": int(sum(4 * g.n for g in graphs))},
+        "batched_vs_plain": {"batched_graphs_per_s": len(graphs) / s, "plain_graphs_per_s": len(graphs) / plain_s,
+                             "speedup": plain_s / s, "same_results": same},
+        "gpu_launches": None, "roofline": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_served(args, world, rank, local):
+    """Serving loop: an open-loop Poisson stream submitted at its arrival
+    times; latency = submit to result. Compared with the same requests run one
+    after another through the plain calls."""
+    import threading
+    import gpu_heipa as H
+    wl = WORKLOADS[args.workload]
+    rng = np.random.default_rng(args.seed + 2000 * rank)
+    reqs = []
+    for i in range(wl["count"]):
+        e_t = float(np.exp(rng.uniform(np.log(wl["emin"]), np.log(wl["emax"]))))
+        mapping = rng.uniform() < 0.3
+        n_t = max(64, int(e_t / 5.0))  # about 5 undirected edges per vertex
+        g = mixed_graph(H, rng, n_t, args.seed + i, (1, 100) if mapping else (1, 10))
+        if mapping:
+            hier, dist = MAP_CHOICES[int(rng.integers(0, 3))]
+            if g.vw is None:
+                g = H.Graph(g.xadj, g.adj, g.ew, np.ones(g.n, np.int32))
+            reqs.append(("map", g, (hier, dist)))
+        else:
+            reqs.append(("part", g, int(2 ** rng.integers(1, 10))))
+    gaps = rng.exponential(1.0 / wl["rate"], len(reqs))
+    edges = sum(r[1].m // 2 for r in reqs)
+    srv = H.Server(local, 64 << 30, workers=args.workers)
+    for kind, g, p in reqs[:8]:  # warm-up
+        rid = srv.submit_map(g, p[0], p[1]) if kind == "map" else srv.submit_partition(g, p)
+        srv.wait(rid)
+    ids, lat = [None] * len(reqs), [None] * len(reqs)
+
+    def collector():
+        for i in range(len(reqs)):
+            while ids[i] is None:
+                time.sleep(0.0002)
+            lat[i] = srv.wait(ids[i])
+
+    th = threading.Thread(target=collector)
+    th.start()
+    t0 = time.perf_counter()
+    t_next = t0
+    for i, (kind, g, p) in enumerate(reqs):
+        t_next += gaps[i]
+        d = t_next - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        ids[i] = srv.submit_map(g, p[0], p[1]) if kind == "map" else srv.submit_partition(g, p)
+    th.join()
+    wall = time.perf_counter() - t0
+    srv.close()
+    lats = np.array([x[2] for x in lat])
+    small = np.array([x[2] for x, r in zip(lat, reqs) if r[1].m // 2 < 1000000])
+    ctx = H.Context(local, H.arena_estimate(max(r[1].n for r in reqs), max(r[1].m for r in reqs), True, True))
+    t1 = time.perf_counter()
+    same = True
+    for (kind, g, p), x in zip(reqs, lat):
+        if kind == "map":
+            part, obj = ctx.process_map(g, p[0], p[1])
+        else:
+            part, obj = ctx.partition(g, p)
+        same = same and obj == x[1]
+    plain_s = time.perf_counter() - t1
+    ctx.close()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": "partition_throughput", "value": edges / wall, "unit": "edges/s", "n_gpus": world,
+        "steps": 1, "warmup": 8, "ms_per_step": 1000 * wall, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": wl["desc"], "requests": len(reqs), "undirected_edges": edges,
+                   "workers": args.workers, "timing": "host wall clock from the first arrival to the last result"},
+        "e2e": {"value": edges / wall, "unit": "edges/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "served": {"p50_ms": float(np.percentile(lats, 50)), "p99_ms": float(np.percentile(lats, 99)),
+                   "p99_ms_under_1M_edges": float(np.percentile(small, 99)) if len(small) else None,
+                   "requests_per_s": len(reqs) / wall, "sequential_plain_s": plain_s,
+                   "sequential_plain_requests_per_s": len(reqs) / plain_s, "same_results": same},
+        "gpu_launches": None, "roofline": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args, world, rank, local):
     import gpu_heipa as H
     wl = WORKLOADS[args.workload]
@@ -372,6 +529,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--kernel-timers", action="store_true", help="print every kernel timer to stderr")
+    ap.add_argument("--workers", type=int, default=8, help="concurrent requests (batch / served workloads)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if world > 1:
@@ -379,8 +537,18 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     try:
+        task = WORKLOADS[args.workload]["task"]
         if args.impl == "reference":
-            rc = run_reference(args, world, rank)
+            if task in ("batch", "served"):
+                print(json.dumps({"impl": "reference", "unavailable": "the batched and served workloads have no "
+                                  "CPU restatement; their plain runs on the GPU are the comparison"}), flush=True)
+                rc = 0
+            else:
+                rc = run_reference(args, world, rank)
+        elif task == "batch":
+            rc = run_batch(args, world, rank, local)
+        elif task == "served":
+            rc = run_served(args, world, rank, local)
         else:
             rc = run_ours(args, world, rank, local)
     finally:
