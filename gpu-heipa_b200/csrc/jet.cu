@@ -17,6 +17,13 @@ constexpr int JW_BLOCK = 128;      // 4 warps per block
 constexpr u32 JB_SLOTS = 16384;    // largest per-block table (128 KB)
 constexpr int JB_BLOCK = 512;
 constexpr u32 EMPTY = NO_BLOCK_ID;
+// Hub rows (more than JW_DEG entries) of the table-based passes are cut into
+// HUB_CHUNK-entry chunks, one warp each, when tables are direct-indexed and
+// k <= HUB_K; the chunks' partial connectivity is summed per row in global
+// memory and the last chunk to finish completes the row.
+constexpr u32 HUB_CHUNK = 4096;
+constexpr u32 HUB_K = 256;
+constexpr int ST_CHUNKS = 8;  // status slot: hub chunk items of the current pass
 constexpr u32 NOKEY = 0xFFFFFFFFu;
 // During perform, map[] holds the new label of every vertex and the MOVED
 // bit marks the vertices that changed block in this iteration; their old
@@ -52,6 +59,9 @@ struct JArgs {
     unsigned long long *items;  // chunk work items (afterburner, delta): (vertex << 32) | chunk
     u32 items_cap;
     unsigned long long inval_all_min;  // moved-row entries from which perform resets every cache
+    s32 *hubacc;  // hub rows: k partial-connectivity sums per row slot (zero between uses), or null
+    u32 *hubcnt;  // hub rows: finished chunks per row slot (zero between uses)
+    u32 hub_cap;  // row slots of hubacc / hubcnt
     s32 *abacc;  // afterburner partial sums of multi-chunk rows (zero between uses)
     u32 *abcnt;  // afterburner finished chunks of multi-chunk rows (zero between uses)
     DevStatus *st;
@@ -168,11 +178,10 @@ __device__ __forceinline__ void table_clear(u32 *tk, s32 *tv, u32 mask) {
 // and no compare-and-swap. Four entries per thread are loaded (ids, then
 // labels) before any table update, which keeps four gathers in flight.
 template<bool BLK>
-__device__ __forceinline__ void dtable_build(const JArgs &a, u32 u, s32 *tv) {
+__device__ __forceinline__ void dtable_build_range(const JArgs &a, u32 u, s32 *tv, u32 from, u32 len) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
-    const u32 len = __ldg(&a.g.rowlen[u]);
     const u32 gs = Grp<BLK>::size(), tid = Grp<BLK>::tid();
-    for (u32 t0 = tid; t0 < len; t0 += 4 * gs) {
+    for (u32 t0 = from + tid; t0 < len; t0 += 4 * gs) {
         u32 b[4];
         s32 w[4];
 #pragma unroll
@@ -189,6 +198,11 @@ __device__ __forceinline__ void dtable_build(const JArgs &a, u32 u, s32 *tv) {
             if (b[j] != EMPTY) atomicAdd(&tv[b[j]], w[j]);
     }
     Grp<BLK>::sync();
+}
+
+template<bool BLK>
+__device__ __forceinline__ void dtable_build(const JArgs &a, u32 u, s32 *tv) {
+    dtable_build_range<BLK>(a, u, tv, 0, __ldg(&a.g.rowlen[u]));
 }
 
 template<bool BLK>
@@ -325,10 +339,10 @@ __device__ __forceinline__ void lp_thread(const JArgs &a, u32 u, u32 ratio) {
     }
 }
 
+// Best block of u from its built connectivity table T (clears T).
 template<bool BLK, bool DIRECT>
-__device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT> T,
-                                         unsigned long long *smu, long long *sms) {
-    T.build(a, u);
+__device__ __forceinline__ void lp_finish_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT> T,
+                                                unsigned long long *smu, long long *sms) {
     const u32 o = a.map[u];
     unsigned long long bk = 0;
     long long own = 0;
@@ -360,6 +374,13 @@ __device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, ConnT
         else lp_finish_map(a, u, bk);
     }
     T.clear();
+}
+
+template<bool BLK, bool DIRECT>
+__device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT> T,
+                                         unsigned long long *smu, long long *sms) {
+    T.build(a, u);
+    lp_finish_group<BLK, DIRECT>(a, u, ratio, T, smu, sms);
 }
 
 // Direct-indexed tables are used when k fits the table and, for the mapping
@@ -409,6 +430,56 @@ __device__ __forceinline__ void block_count(u32 *cnt, unsigned long long *sum, u
     }
 }
 
+// Neighbour-loop kernels (afterburner, delta): rows up to CHUNK_THREAD_MAX
+// entries are handled by one thread; longer rows are cut into chunks of
+// CHUNK entries, one warp each, so that hub rows spread over the whole GPU.
+constexpr u32 CHUNK_THREAD_MAX = 32;
+constexpr u32 CHUNK = 1024;
+
+__device__ __forceinline__ u32 chunks_of(u32 len) { return (len + CHUNK - 1) / CHUNK; }
+
+// Appends nch chunk items of row u (all lanes of the warp call this; lanes
+// with nch == 0 append nothing). One atomic per warp reserves the slots.
+__device__ __forceinline__ void warp_emit_chunks(const JArgs &a, u32 u, u32 nch, u32 *counter) {
+    u32 incl = nch;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const u32 y = __shfl_up_sync(FULL, incl, o);
+        if (lane_id() >= o) incl += y;
+    }
+    const u32 wtot = __shfl_sync(FULL, incl, 31);
+    u32 wbase = 0;
+    if (lane_id() == 31 && wtot) wbase = atomicAdd(counter, wtot);
+    wbase = __shfl_sync(FULL, wbase, 31);
+    const u32 first = wbase + incl - nch;
+    for (u32 c = 0; c < nch; ++c) {
+        if (first + c < a.items_cap) a.items[first + c] = ((unsigned long long) u << 32) | c;
+        else set_error(&a.st->err, DEV_ERR_RANGE);
+    }
+}
+
+// Entries [from, to) of chunk item `it`.
+__device__ __forceinline__ void chunk_range(const JArgs &a, unsigned long long it, u32 &u, u32 &from, u32 &to,
+                                            u32 &nch) {
+    u = (u32) (it >> 32);
+    from = (u32) it * CHUNK;
+    const u32 len = __ldg(&a.g.rowlen[u]);
+    to = len - from < CHUNK ? len : from + CHUNK;
+    nch = chunks_of(len);
+}
+
+// Chunk items of a hub row in row slot h (warp-collective; lanes with len 0
+// emit nothing). Slots beyond the accumulator capacity are reported as an
+// error and skipped.
+__device__ __forceinline__ void emit_hub_chunks(const JArgs &a, u32 h, u32 len) {
+    u32 nch = len ? (len + HUB_CHUNK - 1) / HUB_CHUNK : 0u;
+    if (nch && h >= a.hub_cap) {
+        set_error(&a.st->err, DEV_ERR_RANGE);
+        nch = 0;
+    }
+    warp_emit_chunks(a, h, nch, &a.st->cnt[ST_CHUNKS]);
+}
+
 __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
     const u64 stride = (u64) gridDim.x * blockDim.x;
     u32 nrec = 0;
@@ -432,6 +503,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
+        if (a.hubacc) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
     }
     block_count(&a.st->cnt[ST_AUX], (unsigned long long *) &a.st->sum[4], nrec, erec);
 }
@@ -507,44 +579,6 @@ __global__ void __launch_bounds__(BLOCK) k_lp_filter(JArgs a) {
 
 // afterburner (:269-331 / ProMap :273-320): contribution of neighbour v.
 
-// Neighbour-loop kernels (afterburner, delta): rows up to CHUNK_THREAD_MAX
-// entries are handled by one thread; longer rows are cut into chunks of
-// CHUNK entries, one warp each, so that hub rows spread over the whole GPU.
-constexpr u32 CHUNK_THREAD_MAX = 32;
-constexpr u32 CHUNK = 1024;
-
-__device__ __forceinline__ u32 chunks_of(u32 len) { return (len + CHUNK - 1) / CHUNK; }
-
-// Appends nch chunk items of row u (all lanes of the warp call this; lanes
-// with nch == 0 append nothing). One atomic per warp reserves the slots.
-__device__ __forceinline__ void warp_emit_chunks(const JArgs &a, u32 u, u32 nch) {
-    u32 incl = nch;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const u32 y = __shfl_up_sync(FULL, incl, o);
-        if (lane_id() >= o) incl += y;
-    }
-    const u32 wtot = __shfl_sync(FULL, incl, 31);
-    u32 wbase = 0;
-    if (lane_id() == 31 && wtot) wbase = atomicAdd(&a.st->cnt[ST_HEAVY], wtot);
-    wbase = __shfl_sync(FULL, wbase, 31);
-    const u32 first = wbase + incl - nch;
-    for (u32 c = 0; c < nch; ++c) {
-        if (first + c < a.items_cap) a.items[first + c] = ((unsigned long long) u << 32) | c;
-        else set_error(&a.st->err, DEV_ERR_RANGE);
-    }
-}
-
-// Entries [from, to) of chunk item `it`.
-__device__ __forceinline__ void chunk_range(const JArgs &a, unsigned long long it, u32 &u, u32 &from, u32 &to,
-                                            u32 &nch) {
-    u = (u32) (it >> 32);
-    from = (u32) it * CHUNK;
-    const u32 len = __ldg(&a.g.rowlen[u]);
-    to = len - from < CHUNK ? len : from + CHUNK;
-    nch = chunks_of(len);
-}
-
 // Sum of the afterburner terms over entries [from, to) of u's row, strided
 // over a group of threads (wrap-around s32 arithmetic). The gains, targets
 // and labels read here are not written by the afterburner kernels, so they
@@ -615,7 +649,7 @@ __global__ void __launch_bounds__(BLOCK) k_ab_thread(JArgs a) {
                 nch = chunks_of(len);
             }
         }
-        warp_emit_chunks(a, u, nch);
+        warp_emit_chunks(a, u, nch, &a.st->cnt[ST_HEAVY]);
         const u32 s3 = block_append(&a.st->cnt[ST_MOVES], lock, sm);
         if (lock) a.moves[s3] = u;
     }
@@ -756,7 +790,7 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
             if (len <= CHUNK_THREAD_MAX) acc += delta_range(a, u, 0, len, 0, 1, inval);
             else nch = chunks_of(len);
         }
-        warp_emit_chunks(a, u, nch);
+        warp_emit_chunks(a, u, nch, &a.st->cnt[ST_HEAVY]);
     }
     block_add_s64(acc, &a.st->sum[SUM_DELTA]);
 }
@@ -909,9 +943,8 @@ __device__ __forceinline__ void rb_thread(const JArgs &a, const RbArgs &r, u32 u
 }
 
 template<bool STRONG, bool BLK, bool DIRECT>
-__device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u, ConnTable<BLK, DIRECT> T,
-                                         unsigned long long *smu, long long *sms) {
-    T.build(a, u);
+__device__ __forceinline__ void rb_finish_group(const JArgs &a, const RbArgs &r, u32 u, ConnTable<BLK, DIRECT> T,
+                                                unsigned long long *smu, long long *sms) {
     const u32 o = a.map[u];
     long long own = 0, sum = 0, count = 0;
     unsigned long long bk = 0;
@@ -948,6 +981,13 @@ __device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u,
     T.clear();
 }
 
+template<bool STRONG, bool BLK, bool DIRECT>
+__device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u, ConnTable<BLK, DIRECT> T,
+                                         unsigned long long *smu, long long *sms) {
+    T.build(a, u);
+    rb_finish_group<STRONG, BLK, DIRECT>(a, r, u, T, smu, sms);
+}
+
 template<bool STRONG>
 __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
     const s32 maxv = a.st->imax[1];
@@ -969,6 +1009,7 @@ __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
+        if (a.hubacc) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
     }
 }
 
@@ -1006,6 +1047,56 @@ __global__ void __launch_bounds__(JB_BLOCK) k_rb_block(JArgs a, RbArgs r) {
         const u32 mask = table_mask_for(a.g.rowlen[u], a.k, a.blk_slots);
         if (direct) rb_group<STRONG, true, true>(a, r, u, ConnTable<true, true>{tk, tv, mask, a.k}, smu, sms);
         else rb_group<STRONG, true, false>(a, r, u, ConnTable<true, false>{tk, tv, mask, a.k}, smu, sms);
+    }
+}
+
+// Hub rows in chunks (KIND 0: Jet gain, 1: weak pick, 2: strong pick). A
+// warp aggregates its chunk in a direct-indexed table, adds the non-zero sums
+// to the row's accumulator in global memory, and counts itself finished after
+// a fence; the warp that finishes last reads the full row back (bypassing L1),
+// resets the accumulator and completes the row with the ordinary finishing
+// code. No warp waits for another.
+template<int KIND>
+__global__ void __launch_bounds__(JW_BLOCK) k_hub(JArgs a, u32 ratio, RbArgs r) {
+    u32 *w = warp_table<true>(a.k);
+    s32 *tv = (s32 *) w;
+    const ConnTable<false, true> T{w, tv, 0, a.k};
+    u32 total = a.st->cnt[ST_CHUNKS];
+    if (total > a.items_cap) total = a.items_cap;
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    const u32 lane = lane_id();
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const unsigned long long it = a.items[i];
+        const u32 h = (u32) (it >> 32);
+        const u32 u = a.heavy2[h];
+        const u32 len = __ldg(&a.g.rowlen[u]);
+        const u32 from = (u32) it * HUB_CHUNK;
+        const u32 to = len - from < HUB_CHUNK ? len : from + HUB_CHUNK;
+        const u32 nch = (len + HUB_CHUNK - 1) / HUB_CHUNK;
+        dtable_build_range<false>(a, u, tv, from, to);
+        s32 *acc = a.hubacc + (u64) h * a.k;
+        for (u32 b = lane; b < a.k; b += 32) {
+            const s32 v = tv[b];
+            if (v) {
+                atomicAdd(&acc[b], v);
+                tv[b] = 0;
+            }
+        }
+        __threadfence();
+        __syncwarp();
+        u32 last = 0;
+        if (lane == 0) last = atomicAdd(&a.hubcnt[h], 1u) == nch - 1 ? 1u : 0u;
+        last = __shfl_sync(FULL, last, 0);
+        if (!last) continue;
+        __threadfence();
+        for (u32 b = lane; b < a.k; b += 32) {
+            tv[b] = __ldcg(&acc[b]);
+            acc[b] = 0;
+        }
+        if (lane == 0) a.hubcnt[h] = 0;
+        __syncwarp();
+        if (KIND == 0) lp_finish_group<false, true>(a, u, ratio, T, nullptr, nullptr);
+        else rb_finish_group<KIND == 2, false, true>(a, r, u, T, nullptr, nullptr);
     }
 }
 
@@ -1250,6 +1341,9 @@ JArgs make_args(JetLevel &L) {
     a.items_cap = L.items_cap;
     a.abacc = L.abacc;
     a.inval_all_min = L.cache_pure ? (L.g.m + 1) / 2 : ~0ull;
+    a.hubacc = L.hubacc;
+    a.hubcnt = L.hubcnt;
+    a.hub_cap = L.hub_cap;
     a.abcnt = L.abcnt;
     a.st = L.ctx->d_status;
     a.blk_slots = L.blk_slots;
@@ -1371,14 +1465,6 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     moves = c.balloc<u32>(n);
     heavy = c.balloc<u32>(n);
     heavy2 = c.balloc<u32>(n);
-    // chunk items (afterburner candidates, delta moves; each vertex at most
-    // once): one per row of <= CHUNK entries, so at most n + m / CHUNK + 1
-    items_cap = (u32) std::min<u64>(0xFFFFFFFFull, (u64) n + g.m / CHUNK + 1);
-    items = c.balloc<unsigned long long>(items_cap);
-    abacc = c.balloc<s32>(n);
-    abcnt = c.balloc<u32>(n);
-    HP_CUDA(cudaMemsetAsync(abacc, 0, sizeof(s32) * n, c.stream));
-    HP_CUDA(cudaMemsetAsync(abcnt, 0, sizeof(u32) * n, c.stream));
     blk_slots = block_slots_for(k);
     // warp tier: direct-indexed table of k values when k is small enough
     // (for the mapping objective the candidate scoring loops over the table,
@@ -1386,6 +1472,26 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     warp_direct = k <= JW_SLOTS && (d == nullptr || k <= 256);
     warp_slots = warp_direct ? k : JW_SLOTS;
     warp_smem = (JW_BLOCK / 32) * (warp_direct ? 1u : 2u) * warp_slots * (u32) sizeof(u32);
+    // chunk items (afterburner candidates, delta moves; each vertex at most
+    // once): one per row of <= CHUNK entries, so at most n + m / CHUNK + 1
+    items_cap = (u32) std::min<u64>(0xFFFFFFFFull, (u64) n + g.m / CHUNK + 1);
+    items = c.balloc<unsigned long long>(items_cap);
+    // hub-row accumulators (rows of more than JW_DEG entries: fewer than
+    // m / JW_DEG + 1 of them) when the tables are direct-indexed and k small
+    hubacc = nullptr;
+    hubcnt = nullptr;
+    hub_cap = 0;
+    if (warp_direct && k <= HUB_K) {
+        hub_cap = (u32) std::min<u64>(n, g.m / JW_DEG + 1);
+        hubacc = c.balloc<s32>((u64) hub_cap * k);
+        hubcnt = c.balloc<u32>(hub_cap);
+        HP_CUDA(cudaMemsetAsync(hubacc, 0, sizeof(s32) * (u64) hub_cap * k, c.stream));
+        HP_CUDA(cudaMemsetAsync(hubcnt, 0, sizeof(u32) * hub_cap, c.stream));
+    }
+    abacc = c.balloc<s32>(n);
+    abcnt = c.balloc<u32>(n);
+    HP_CUDA(cudaMemsetAsync(abacc, 0, sizeof(s32) * n, c.stream));
+    HP_CUDA(cudaMemsetAsync(abcnt, 0, sizeof(u32) * n, c.stream));
     HP_CUDA(cudaMemcpyAsync(map, part, sizeof(u32) * n, cudaMemcpyDeviceToDevice, c.stream));
     device_fill<u32>(c, dest_cache, n, NULL_PART);
     HP_CUDA(cudaMemsetAsync(gain_cache, 0, sizeof(s32) * n, c.stream));
@@ -1417,7 +1523,13 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     }
     {
         KernTimer kt(c, "k_lp_block");
-        k_lp_block<<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, ratio_pct); note_launch();
+        if (hubacc) {
+            k_hub<0><<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(
+                a, ratio_pct, RbArgs{});
+        } else {
+            k_lp_block<<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, ratio_pct);
+        }
+        note_launch();
     }
     HP_LAUNCH_CHECK();
     c.instr.end(c.stream, gain_rec);
@@ -1482,7 +1594,13 @@ void JetLevel::weak() {
         }
         {
             KernTimer kt1(c, "k_weak_block");
-            k_rb_block<false><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+            if (hubacc) {
+                k_hub<1><<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
+                               c.stream>>>(a, 0u, r);
+            } else {
+                k_rb_block<false><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r);
+            }
+            note_launch();
         }
     }
     ProfScope p3(c, "weak.order");
@@ -1548,7 +1666,13 @@ void JetLevel::strong() {
         }
         {
             KernTimer kt1(c, "k_strong_block");
-            k_rb_block<true><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r); note_launch();
+            if (hubacc) {
+                k_hub<2><<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
+                               c.stream>>>(a, 0u, r);
+            } else {
+                k_rb_block<true><<<c.sm_count * 4, JB_BLOCK, blk_slots * 8, c.stream>>>(a, r);
+            }
+            note_launch();
         }
     }
     ProfScope p3(c, "strong.order");

@@ -64,6 +64,9 @@ struct JetLevel {
     u32 *heavy2 = nullptr;
     unsigned long long *items = nullptr;  // chunk work items (afterburner, delta)
     u32 items_cap = 0;
+    s32 *hubacc = nullptr;  // hub-row connectivity accumulators (direct tables, small k), or null
+    u32 *hubcnt = nullptr;  // hub-row finished-chunk counters
+    u32 hub_cap = 0;        // hub-row slots
     s32 *abacc = nullptr;  // afterburner partial sums of multi-chunk rows
     u32 *abcnt = nullptr;  // afterburner finished-chunk counts of multi-chunk rows
     u32 blk_slots = 0;  // block-tier table size
