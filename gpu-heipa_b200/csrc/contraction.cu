@@ -18,8 +18,11 @@ constexpr u32 C_WARP_SLOTS = 1u << C_WARP_BITS;
 constexpr u32 C_BLOCK_MAX = 4096;
 constexpr u32 C_BLOCK_BITS = 13;  // 8192 slots per block
 constexpr u32 C_BLOCK_SLOTS = 1u << C_BLOCK_BITS;
+constexpr u32 C_BLOCK_SMALL_MAX = 1024;  // block tier with a 2048-slot table (16 KB) up to this capacity
+constexpr u32 C_BLOCK_SMALL_BITS = 11;
 constexpr int C_WARP_BLOCK = 128;  // 4 warps per block for the warp kernel
 constexpr int C_HUGE_BLOCK = 1024;
+constexpr int C_ST_BLOCK_LARGE = 3;  // status slot: clusters of the large block tier
 
 __device__ __forceinline__ u32 hslot(u32 key, u32 bits) { return (key * 2654435761u) >> (32 - bits); }
 
@@ -51,8 +54,16 @@ struct CArgs {
 
 // Thread-per-coarse-vertex aggregation in registers for capacities <= 16;
 // larger coarse vertices are appended to the warp / block / huge lists.
-__global__ void k_contract_small(CArgs a, u32 *wl, u32 *wcnt, u32 *bl, u32 *bcnt, u32 *hl, u32 *hcnt, u32 *hoff,
-                                 unsigned long long *hbump) {
+struct TierLists {
+    u32 *wl, *wcnt;    // warp tier
+    u32 *bl, *bcnt;    // block tier, 2048-slot tables
+    u32 *bl2, *b2cnt;  // block tier, 8192-slot tables
+    u32 *hl, *hcnt;    // huge clusters
+    u32 *hoffc;        // per coarse vertex: offset of its global table (huge clusters)
+    unsigned long long *hbump;  // global table slots handed out
+};
+
+__global__ void k_contract_small(CArgs a, TierLists L) {
     const u64 stride = (u64) gridDim.x * blockDim.x;
     unsigned long long msum = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.c.n; base += stride) {
@@ -61,37 +72,44 @@ __global__ void k_contract_small(CArgs a, u32 *wl, u32 *wcnt, u32 *bl, u32 *bcnt
         u32 cap = 0;
         if (c < a.c.n) {
             cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
-            if (cap <= C_THREAD_MAX) {
+            const u32 m0 = a.moff[c], mc = a.moff[c + 1] - m0;
+            if (cap <= C_THREAD_MAX && mc <= 2) {
+                // matched clusters have one or two members: the (at most 16)
+                // entries of their rows are loaded first, then all coarse ids
+                // are gathered at once, then aggregated in registers (larger
+                // clusters of a caller-given mapping go to the warp tier)
+                const u32 u0 = a.mlist[m0];
+                const u32 u1 = mc > 1 ? a.mlist[m0 + 1] : u0;
+                const u64 b0 = a.g.rowptr[u0], b1 = a.g.rowptr[u1];
+                const u32 l0 = a.g.rowlen[u0], l1 = mc > 1 ? a.g.rowlen[u1] : 0u;
                 u32 keys[C_THREAD_MAX];
                 s32 ws[C_THREAD_MAX];
 #pragma unroll
                 for (int s = 0; s < (int) C_THREAD_MAX; ++s) {
+                    const u32 t = (u32) s;
                     keys[s] = EMPTY;
                     ws[s] = 0;
-                }
-                for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
-                    const u32 u = a.mlist[mi];
-                    const u64 beg = a.g.rowptr[u];
-                    const u32 len = a.g.rowlen[u];
-                    for (u32 t = 0; t < len; ++t) {
-                        const u32 cv = a.map[a.g.adj[beg + t]];
-                        if (cv == c) continue;
-                        const s32 w = g_ew(a.g, beg + t);
-                        bool done = false;
-#pragma unroll
-                        for (int s = 0; s < (int) C_THREAD_MAX; ++s)
-                            if (!done && keys[s] == cv) {
-                                ws[s] = wadd(ws[s], w);
-                                done = true;
-                            }
-#pragma unroll
-                        for (int s = 0; s < (int) C_THREAD_MAX; ++s)
-                            if (!done && keys[s] == EMPTY) {
-                                keys[s] = cv;
-                                ws[s] = w;
-                                done = true;
-                            }
+                    if (t < l0 + l1) {
+                        const u64 e = t < l0 ? b0 + t : b1 + (t - l0);
+                        keys[s] = __ldg(&a.g.adj[e]);
+                        ws[s] = g_ew(a.g, e);
                     }
+                }
+#pragma unroll
+                for (int s = 0; s < (int) C_THREAD_MAX; ++s)
+                    if (keys[s] != EMPTY) {
+                        keys[s] = __ldg(&a.map[keys[s]]);
+                        if (keys[s] == c) keys[s] = EMPTY;  // self loop
+                    }
+                // merge equal coarse ids into their first occurrence
+#pragma unroll
+                for (int s = 1; s < (int) C_THREAD_MAX; ++s) {
+#pragma unroll
+                    for (int t = 0; t < s; ++t)
+                        if (keys[s] != EMPTY && keys[t] == keys[s]) {
+                            ws[t] = wadd(ws[t], ws[s]);
+                            keys[s] = EMPTY;
+                        }
                 }
                 u64 pos = a.c.rowptr[c];
                 u32 cntu = 0;
@@ -105,25 +123,64 @@ __global__ void k_contract_small(CArgs a, u32 *wl, u32 *wcnt, u32 *bl, u32 *bcnt
                 a.c.rowlen[c] = cntu;
                 msum += cntu;
             } else if (cap <= C_WARP_MAX) {
-                cls = 1;
-            } else if (cap <= C_BLOCK_MAX) {
+                cls = 1;  // includes small clusters of more than two members
+            } else if (cap <= C_BLOCK_SMALL_MAX) {
                 cls = 2;
+            } else if (cap <= C_BLOCK_MAX) {
+                cls = 4;
             } else {
                 cls = 3;
+                L.hoffc[c] = (u32) atomicAdd(L.hbump, (unsigned long long) (2 * cap));
             }
         }
-        u32 s1 = warp_append(wcnt, cls == 1);
-        if (cls == 1) wl[s1] = c;
-        u32 s2 = warp_append(bcnt, cls == 2);
-        if (cls == 2) bl[s2] = c;
-        u32 s3 = warp_append(hcnt, cls == 3);
-        if (cls == 3) {
-            hl[s3] = c;
-            hoff[s3] = (u32) atomicAdd(hbump, (unsigned long long) (2 * cap));
-        }
+        u32 s1 = warp_append(L.wcnt, cls == 1);
+        if (cls == 1) L.wl[s1] = c;
+        u32 s2 = warp_append(L.bcnt, cls == 2);
+        if (cls == 2) L.bl[s2] = c;
+        u32 s4 = warp_append(L.b2cnt, cls == 4);
+        if (cls == 4) L.bl2[s4] = c;
+        u32 s3 = warp_append(L.hcnt, cls == 3);
+        if (cls == 3) L.hl[s3] = c;
     }
     msum = warp_sum<unsigned long long>(msum);
     if (lane_id() == 0 && msum) atomicAdd(a.m_out, msum);
+}
+
+// Calls insert(cv, w) for every entry of the member rows of cluster c whose
+// coarse neighbour cv differs from c; entries are strided over a group of
+// `nt` threads starting at `tid` across the concatenated member rows (one or
+// two members), four entries per thread loaded before they are inserted.
+template<typename Insert>
+__device__ __forceinline__ void for_cluster_entries(const CArgs &a, u32 c, u32 tid, u32 nt, Insert insert) {
+    const u32 m0 = a.moff[c], mc = a.moff[c + 1] - m0;
+    for (u32 mi = 0; mi < mc; mi += 2) {
+        const u32 u0 = a.mlist[m0 + mi];
+        const u32 u1 = mi + 1 < mc ? a.mlist[m0 + mi + 1] : u0;
+        const u64 b0 = a.g.rowptr[u0], b1 = a.g.rowptr[u1];
+        const u32 l0 = a.g.rowlen[u0], l1 = mi + 1 < mc ? a.g.rowlen[u1] : 0u;
+        const u32 total = l0 + l1;
+        for (u32 t0 = tid; t0 < total; t0 += 4 * nt) {
+            u32 cv[4];
+            s32 w[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const u32 t = t0 + j * nt;
+                cv[j] = EMPTY;
+                w[j] = 0;
+                if (t < total) {
+                    const u64 e = t < l0 ? b0 + t : b1 + (t - l0);
+                    cv[j] = __ldg(&a.g.adj[e]);
+                    w[j] = g_ew(a.g, e);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (cv[j] != EMPTY) cv[j] = __ldg(&a.map[cv[j]]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (cv[j] != EMPTY && cv[j] != c) insert(cv[j], w[j]);
+        }
+    }
 }
 
 // Inserts (cv, w) into an open-addressing table with linear probing.
@@ -159,17 +216,9 @@ __global__ void __launch_bounds__(C_WARP_BLOCK) k_contract_warp(CArgs a, const u
         u32 bits = 6;
         while ((1u << bits) < 2 * cap && bits < C_WARP_BITS) ++bits;
         const u32 tsz = 1u << bits;
-        for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
-            const u32 u = a.mlist[mi];
-            const u64 beg = a.g.rowptr[u];
-            const u32 len = a.g.rowlen[u];
-            for (u32 t = lane; t < len; t += 32) {
-                const u32 cv = a.map[a.g.adj[beg + t]];
-                if (cv == c) continue;
-                if (!table_insert(tk, tw, tsz - 1, hslot(cv, bits), cv, g_ew(a.g, beg + t)))
-                    set_error(a.err, DEV_ERR_HASH_FULL);
-            }
-        }
+        for_cluster_entries(a, c, (u32) lane, 32u, [&](u32 cv, s32 w) {
+            if (!table_insert(tk, tw, tsz - 1, hslot(cv, bits), cv, w)) set_error(a.err, DEV_ERR_HASH_FULL);
+        });
         __syncwarp();
         const u64 out = a.c.rowptr[c];
         u32 cntu = 0;
@@ -215,12 +264,13 @@ __device__ __forceinline__ u32 block_emit(u32 *tk, s32 *tw, u32 slots, u64 out, 
     return tot;
 }
 
-__global__ void __launch_bounds__(BLOCK) k_contract_block(CArgs a, const u32 *bl, const u32 *bcnt) {
+__global__ void __launch_bounds__(BLOCK) k_contract_block(CArgs a, const u32 *bl, const u32 *bcnt, u32 max_bits) {
     extern __shared__ u32 dsm[];
+    const u32 slots = 1u << max_bits;
     u32 *tk = dsm;
-    s32 *tw = (s32 *) (dsm + C_BLOCK_SLOTS);
+    s32 *tw = (s32 *) (dsm + slots);
     __shared__ u32 scan_sm[32];
-    for (u32 s = threadIdx.x; s < C_BLOCK_SLOTS; s += blockDim.x) {
+    for (u32 s = threadIdx.x; s < slots; s += blockDim.x) {
         tk[s] = EMPTY;
         tw[s] = 0;
     }
@@ -232,19 +282,11 @@ __global__ void __launch_bounds__(BLOCK) k_contract_block(CArgs a, const u32 *bl
         // table of the next power of two >= 2 * capacity (<= C_BLOCK_SLOTS)
         const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
         u32 bits = 9;
-        while ((1u << bits) < 2 * cap && bits < C_BLOCK_BITS) ++bits;
+        while ((1u << bits) < 2 * cap && bits < max_bits) ++bits;
         const u32 tsz = 1u << bits;
-        for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
-            const u32 u = a.mlist[mi];
-            const u64 beg = a.g.rowptr[u];
-            const u32 len = a.g.rowlen[u];
-            for (u32 t = threadIdx.x; t < len; t += blockDim.x) {
-                const u32 cv = a.map[a.g.adj[beg + t]];
-                if (cv == c) continue;
-                if (!table_insert(tk, tw, tsz - 1, hslot(cv, bits), cv, g_ew(a.g, beg + t)))
-                    set_error(a.err, DEV_ERR_HASH_FULL);
-            }
-        }
+        for_cluster_entries(a, c, threadIdx.x, blockDim.x, [&](u32 cv, s32 w) {
+            if (!table_insert(tk, tw, tsz - 1, hslot(cv, bits), cv, w)) set_error(a.err, DEV_ERR_HASH_FULL);
+        });
         __syncthreads();
         const u32 cntu = block_emit(tk, tw, tsz, a.c.rowptr[c], a.c.adj, a.c.ew, scan_sm);
         if (threadIdx.x == 0) a.c.rowlen[c] = cntu;
@@ -267,8 +309,8 @@ __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u
         const u32 c = hl[i];
         const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
         const u32 tsz = 2 * cap;
-        u32 *tk = tkeys + hoff[i];
-        s32 *tw = twts + hoff[i];
+        u32 *tk = tkeys + hoff[c];
+        s32 *tw = twts + hoff[c];
         for (u32 s = threadIdx.x; s < tsz; s += blockDim.x) {
             tk[s] = EMPTY;
             tw[s] = 0;
@@ -340,8 +382,9 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     u32 *mlist = ctx.balloc<u32>(g.n);
     u32 *wl = ctx.balloc<u32>(n_c);
     u32 *bl = ctx.balloc<u32>(n_c);
+    u32 *bl2 = ctx.balloc<u32>(n_c);
     u32 *hl = ctx.balloc<u32>(n_c);
-    u32 *hoff = ctx.balloc<u32>(n_c);
+    u32 *hoffc = ctx.balloc<u32>(n_c);
     HP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(u32) * n_c, ctx.stream));
     HP_CUDA(cudaMemsetAsync(capsum, 0, sizeof(u32) * n_c, ctx.stream));
     HP_CUDA(cudaMemsetAsync(c.vw, 0, sizeof(s32) * n_c, ctx.stream));
@@ -365,32 +408,48 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     DevStatus *st = ctx.d_status;
     CArgs a{g, mapping, moff, mlist, c, &st->err, (unsigned long long *) &st->sum[1]};
     const size_t rec0 = ctx.instr.begin(ctx.stream, "contract", 0.0);
-    k_contract_small<<<ctx.grid(n_c, BLOCK), BLOCK, 0, ctx.stream>>>(
-        a, wl, &st->cnt[0], bl, &st->cnt[1], hl, &st->cnt[2], hoff, (unsigned long long *) &st->sum[0]); note_launch();
+    const size_t rec_t = ctx.instr.begin(ctx.stream, "contract_thread", 0.0);
+    TierLists TL{wl, &st->cnt[0], bl, &st->cnt[1], bl2, &st->cnt[C_ST_BLOCK_LARGE], hl, &st->cnt[2], hoffc,
+                 (unsigned long long *) &st->sum[0]};
+    k_contract_small<<<ctx.grid(n_c, BLOCK), BLOCK, 0, ctx.stream>>>(a, TL); note_launch();
     HP_LAUNCH_CHECK();
+    ctx.instr.end(ctx.stream, rec_t);
     ctx.instr.end(ctx.stream, rec0);
     const DevStatus &s1 = ctx.read_status();
-    const u32 nw = s1.cnt[0], nb = s1.cnt[1], nh = s1.cnt[2];
+    const u32 nw = s1.cnt[0], nb = s1.cnt[1], nh = s1.cnt[2], nb2 = s1.cnt[C_ST_BLOCK_LARGE];
     const u64 hslots = (u64) s1.sum[0];
     if (nw) {
         KernTimer kt(ctx, "contract");
+        KernTimer kt1(ctx, "contract_warp");
         k_contract_warp<<<ctx.grid((u64) nw * 32, C_WARP_BLOCK), C_WARP_BLOCK, 0, ctx.stream>>>(a, wl, &st->cnt[0]); note_launch();
         HP_LAUNCH_CHECK();
     }
     if (nb) {
+        // clusters of up to C_BLOCK_SMALL_MAX entries: 16 KB tables, so
+        // eight 256-thread blocks fit on an SM
+        const size_t smem = ((size_t) 1 << C_BLOCK_SMALL_BITS) * 8;
+        KernTimer kt(ctx, "contract");
+        KernTimer kt1(ctx, "contract_block");
+        k_contract_block<<<(u32) std::min<u64>(nb, (u64) ctx.sm_count * 8), BLOCK, smem, ctx.stream>>>(
+            a, bl, &st->cnt[1], C_BLOCK_SMALL_BITS); note_launch();
+        HP_LAUNCH_CHECK();
+    }
+    if (nb2) {
         const size_t smem = (size_t) C_BLOCK_SLOTS * 8;
         HP_CUDA(cudaFuncSetAttribute(k_contract_block, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
         KernTimer kt(ctx, "contract");
-        k_contract_block<<<(u32) std::min<u64>(nb, (u64) ctx.sm_count * 3), BLOCK, smem, ctx.stream>>>(a, bl,
-                                                                                                     &st->cnt[1]); note_launch();
+        KernTimer kt1(ctx, "contract_block");
+        k_contract_block<<<(u32) std::min<u64>(nb2, (u64) ctx.sm_count * 3), BLOCK, smem, ctx.stream>>>(
+            a, bl2, &st->cnt[C_ST_BLOCK_LARGE], C_BLOCK_BITS); note_launch();
         HP_LAUNCH_CHECK();
     }
     if (nh) {
         u32 *tkeys = ctx.balloc<u32>(hslots);
         s32 *twts = ctx.balloc<s32>(hslots);
         KernTimer kt(ctx, "contract");
+        KernTimer kt1(ctx, "contract_huge");
         k_contract_huge<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
-            a, hl, &st->cnt[2], hoff, tkeys, twts); note_launch();
+            a, hl, &st->cnt[2], hoffc, tkeys, twts); note_launch();
         HP_LAUNCH_CHECK();
     }
     const DevStatus &s2 = ctx.read_status();

@@ -52,6 +52,29 @@ def test_contract_parity(ctx, name, g):
     np.testing.assert_array_equal(cg.vw, ov)
 
 
+@pytest.mark.parametrize("group", [3, 4, 7])
+def test_contract_parity_large_clusters(ctx, group):
+    # a caller-given mapping with clusters of more than two members
+    g = H.Graph.rmat(12, 8, seed=9)
+    mapping = (np.arange(g.n) // group).astype(np.uint32)
+    n_c = int(mapping.max()) + 1
+    dg = ctx.upload(g)
+    try:
+        dc = ctx.contract(dg, mapping, n_c)
+        cg = dc.download()
+        dc.free()
+    finally:
+        dg.free()
+    oc = O.contract(to_oracle(g), mapping, n_c)
+    ox, oa, oe, ov = oc.arrays()
+    gx, ga, ge = sorted_rows(cg.xadj, cg.adj, cg.ew)
+    ox, oa, oe = sorted_rows(ox, oa, oe)
+    np.testing.assert_array_equal(gx, ox)
+    np.testing.assert_array_equal(ga, oa)
+    np.testing.assert_array_equal(ge, oe)
+    np.testing.assert_array_equal(cg.vw, ov)
+
+
 def test_contract_kat_six_cycle(ctx):
     # 6-cycle with weights 1..6, vertex weights 1..6, clusters {0,3},{1,4},{2,5}
     n = 6
