@@ -3,6 +3,9 @@
 // tie rules documented in jet.cuh (lowest block id on best-block ties,
 // mini-bucket order by vertex id, fallback slots in ascending vertex id).
 #include "jet.cuh"
+
+#include <mutex>
+#include <vector>
 #include "prims.cuh"
 
 #include <algorithm>
@@ -556,9 +559,14 @@ __global__ void __launch_bounds__(JB_BLOCK) k_lp_block(JArgs a, u32 ratio) {
     }
 }
 
-// filter potentially viable moves (:247-258)
+// filter potentially viable moves (:247-258); also resets the list counters
+// of the gain pass for the afterburner that follows (the gain kernels are done)
 __global__ void __launch_bounds__(BLOCK) k_lp_filter(JArgs a) {
     __shared__ u32 sm[33];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.st->cnt[ST_HEAVY] = 0;
+        a.st->cnt[ST_HEAVY2] = 0;
+    }
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
         const u32 u = (u32) (base + threadIdx.x);
@@ -691,14 +699,6 @@ __global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
 
 // ---- perform_moves (:753-924 / ProMap :1103-1216) -----------------------------------
 
-// Clears the MOVED bits set by k_apply once the objective delta is known.
-__global__ void k_unmark(JArgs a) {
-    const u32 total = a.st->cnt[ST_MOVES];
-    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const u32 u = a.moves[i];
-        a.map[u] &= ~MOVED;
-    }
-}
 
 
 // Invalidates the caches of the neighbours in entries [from, to) of u's row
@@ -757,10 +757,27 @@ __device__ __forceinline__ bool scattered_inval(const JArgs &a) {
     return (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] < a.inval_all_min;
 }
 
-__global__ void k_inval_all(JArgs a) {
-    if (scattered_inval(a)) return;
-    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < a.g.n; u += gridDim.x * blockDim.x)
-        a.dest_cache[u] = NULL_PART;
+// Last perform kernel: resets every cache when the delta pass skipped the
+// scattered resets, and clears the moved bits.
+__global__ void k_inval_unmark(JArgs a) {
+    if (!scattered_inval(a))
+        for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < a.g.n; u += gridDim.x * blockDim.x)
+            a.dest_cache[u] = NULL_PART;
+    const u32 total = a.st->cnt[ST_MOVES];
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const u32 u = a.moves[i];
+        a.map[u] &= ~MOVED;
+    }
+}
+
+// First perform kernel: clears the counters and sums perform accumulates.
+__global__ void k_perform_reset(DevStatus *st) {
+    if (threadIdx.x == 0) {
+        st->cnt[ST_HEAVY] = 0;
+        st->cnt[ST_HEAVY2] = 0;
+        st->sum[SUM_DELTA] = 0;
+        st->sum[SUM_PERF_ENTRIES] = 0;
+    }
 }
 
 // Adds a per-thread s64 to the status word with one atomic per block.
@@ -793,6 +810,20 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
         warp_emit_chunks(a, u, nch, &a.st->cnt[ST_HEAVY]);
     }
     block_add_s64(acc, &a.st->sum[SUM_DELTA]);
+    if (blockIdx.x == 0) {
+        // maximum block weight after the moves (k_apply has finished)
+        __shared__ s32 mx[32];
+        s32 m = 0;
+        for (u32 b = threadIdx.x; b < a.k; b += blockDim.x) m = a.bw[b] > m ? a.bw[b] : m;
+        m = __reduce_max_sync(FULL, m);
+        if (lane_id() == 0) mx[warp_in_block()] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s32 r = 0;
+            for (u32 w = 0; w < (blockDim.x >> 5); ++w) r = mx[w] > r ? mx[w] : r;
+            a.st->imax[MAX_BW] = r;
+        }
+    }
 }
 
 // Six blocks per SM (at most 40 registers): the pass is bound by dependent
@@ -1192,10 +1223,9 @@ __global__ void k_strong_filter(JArgs a, const u32 *svals, const long long *pref
     }
 }
 
-// cookie cutter (:524-551)
-__global__ void k_cookie(const s32 *bw, u32 k, s32 max_b_w, const long long *B, long long *ea, long long *es,
-                         long long *max_v) {
-    __shared__ long long sm[32];
+// cookie cutter (:524-551), one block
+__device__ __forceinline__ void cookie_block(const s32 *bw, u32 k, s32 max_b_w, const long long *B, long long *ea,
+                                             long long *es, long long *max_v, long long *sm) {
     long long carry = 0, carry2 = 0;
     for (u32 base = 0; base < k; base += blockDim.x) {
         const u32 p = base + threadIdx.x;
@@ -1221,6 +1251,12 @@ __global__ void k_cookie(const s32 *bw, u32 k, s32 max_b_w, const long long *B, 
     }
 }
 
+__global__ void k_cookie(const s32 *bw, u32 k, s32 max_b_w, const long long *B, long long *ea, long long *es,
+                         long long *max_v) {
+    __shared__ long long sm[32];
+    cookie_block(bw, k, max_b_w, B, ea, es, max_v, sm);
+}
+
 __device__ __forceinline__ s32 chunk_of(const long long *es, u32 k, long long tg) {
     // largest id in [0, k] with es[id] <= tg (es non-decreasing, es[0] = 0)
     u32 lo = 0, hi = k + 1;
@@ -1230,6 +1266,22 @@ __device__ __forceinline__ s32 chunk_of(const long long *es, u32 k, long long tg
         else hi = mid;
     }
     return (s32) lo - 1;
+}
+
+// First attempt of one evicted vertex; returns true when it needs a fallback
+// slot.
+__device__ __forceinline__ bool strong_assign_one(const JArgs &a, u32 u, long long mpre_j, const long long *ea,
+                                                  const long long *es) {
+    const u32 o = a.map[u];
+    const long long vw = g_vw(a.g, u);
+    const long long tg = mpre_j - ea[o];
+    const s32 id = chunk_of(es, a.k, tg);
+    if (id < (s32) a.k && vw / 2 <= es[id + 1] - tg) {
+        a.dest_part[u] = (u32) id;
+        return false;
+    }
+    a.dest_part[u] = o;
+    return id < (s32) a.k;
 }
 
 // adjust_scores (:560-584): first attempt for every evicted vertex; those
@@ -1244,16 +1296,7 @@ __global__ void k_strong_assign(JArgs a, const long long *mpre, const long long 
         u32 u = 0;
         if (j < total) {
             u = a.moves[j];
-            const u32 o = a.map[u];
-            const long long vw = g_vw(a.g, u);
-            const long long tg = mpre[j] - ea[o];
-            const s32 id = chunk_of(es, a.k, tg);
-            if (id < (s32) a.k && vw / 2 <= es[id + 1] - tg) {
-                a.dest_part[u] = (u32) id;
-            } else {
-                a.dest_part[u] = o;
-                f = id < (s32) a.k;
-            }
+            f = strong_assign_one(a, u, mpre[j], ea, es);
         }
         const u32 s = warp_append(n_fail, f);
         if (f) fail[s] = u;
@@ -1268,10 +1311,8 @@ __global__ void k_copy_count(u32 *dst, const u32 *src, const u32 *d_count) {
 
 // Fallback slots in ascending vertex order (one thread; at most one
 // straddling vertex per chunk boundary reaches this).
-__global__ void k_strong_fallback(JArgs a, const u32 *fail, const u32 *d_nf, const long long *es, long long *max_v) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const u32 nf = *d_nf;
-    if (nf == 0) return;
+__device__ __forceinline__ void strong_fallback_seq(const JArgs &a, const u32 *fail, u32 nf, const long long *es,
+                                                    long long *max_v) {
     long long mv = *max_v;
     for (u32 i = 0; i < nf; ++i) {
         const u32 u = fail[i];
@@ -1291,6 +1332,190 @@ __global__ void k_strong_fallback(JArgs a, const u32 *fail, const u32 *d_nf, con
         a.dest_part[u] = dest;
     }
     *max_v = mv;
+}
+
+__global__ void k_strong_fallback(JArgs a, const u32 *fail, const u32 *d_nf, const long long *es, long long *max_v) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const u32 nf = *d_nf;
+    if (nf) strong_fallback_seq(a, fail, nf, es, max_v);
+}
+
+__device__ __forceinline__ int bits_for_u32(u32 x) { return x ? 32 - __clz(x) : 0; }
+
+// ---- rebalance ordering of small levels in one block -------------------------------
+
+// Levels of at most ORDER_SMALL_N vertices run the whole ordering of a
+// rebalance step (candidate compaction, stable sort by mini-bucket key,
+// weight prefix, bucket bounds, move selection and, for strong rebalancing,
+// the cookie cutter and slot assignment) in one 1024-thread block instead of
+// ~25 small launches. The block reads and writes its own arrays only, with a
+// __syncthreads() between phases.
+constexpr u32 ORDER_SMALL_N = 4096;
+constexpr int OB = 1024;
+
+struct OrderScratch {
+    u32 *cands, *ck, *cands2, *ck2;
+    long long *prefix, *B;
+    long long *ea, *es, *mpre;  // strong only
+    u32 *fail, *fail2;          // strong only
+};
+
+// Stable LSD radix sort (8-bit digits) of (k0[i], v0[i]), i < cnt, by key bits
+// [0, bits), ping-ponging with (k1, v1); returns true when the result is in
+// (k1, v1). All OB threads call it.
+__device__ bool block_sort_pairs(u32 *k0, u32 *v0, u32 *k1, u32 *v1, u32 cnt, int bits, u32 *offs,
+                                 u32 (*wc)[256], u32 *scan_sm) {
+    const u32 tid = threadIdx.x, w = warp_in_block(), lane = lane_id();
+    const unsigned lt = (1u << lane) - 1u;
+    bool flipped = false;
+    for (int shift = 0; shift < bits; shift += 8) {
+        if (tid < 256) offs[tid] = 0;
+        __syncthreads();
+        for (u32 i = tid; i < cnt; i += OB) atomicAdd(&offs[(k0[i] >> shift) & 255u], 1u);
+        __syncthreads();
+        u32 tot;
+        const u32 v = tid < 256 ? offs[tid] : 0u;
+        const u32 p = block_exclusive_scan<u32>(v, tot, scan_sm);
+        if (tid < 256) offs[tid] = p;
+        __syncthreads();
+        for (u32 base = 0; base < cnt; base += OB) {
+            for (u32 j = tid; j < 32 * 256; j += OB) wc[j >> 8][j & 255] = 0;
+            __syncthreads();
+            const u32 i = base + tid;
+            const bool valid = i < cnt;
+            const u32 key = valid ? k0[i] : 0u;
+            const u32 d = valid ? ((key >> shift) & 255u) : 256u;
+            const unsigned mask = __match_any_sync(FULL, d);
+            if (valid && (u32) (__ffs(mask) - 1) == lane) wc[w][d] = (u32) __popc(mask);
+            __syncthreads();
+            if (valid) {
+                u32 off = offs[d] + (u32) __popc(mask & lt);
+                for (u32 x = 0; x < w; ++x) off += wc[x][d];
+                k1[off] = key;
+                v1[off] = v0[i];
+            }
+            __syncthreads();
+            if (tid < 256) {
+                u32 add = 0;
+                for (u32 x = 0; x < OB / 32; ++x) add += wc[x][tid];
+                offs[tid] += add;
+            }
+            __syncthreads();
+        }
+        u32 *t = k0;
+        k0 = k1;
+        k1 = t;
+        t = v0;
+        v0 = v1;
+        v1 = t;
+        flipped = !flipped;
+    }
+    return flipped;
+}
+
+template<bool STRONG>
+__global__ void __launch_bounds__(OB, 1) k_order_small(JArgs a, RbArgs r, u32 width, int key_bits, OrderScratch S,
+                                                        s32 max_b_w) {
+    __shared__ u32 offs[256];
+    __shared__ u32 wc[OB / 32][256];
+    __shared__ u32 scan_sm[32];
+    __shared__ long long lsm[32];
+    __shared__ u32 cnt_sm[3];  // candidates, moves, fallbacks
+    const u32 tid = threadIdx.x, n = a.g.n;
+    if (tid < 3) cnt_sm[tid] = 0;
+    if (STRONG)
+        for (u32 b = tid; b < a.k; b += OB) S.ea[b] = 0;
+    __syncthreads();
+    // 1. candidates in ascending vertex id with their keys
+    for (u32 base = 0; base < n; base += OB) {
+        const u32 u = base + tid;
+        const bool c = u < n && r.keys[u] != NOKEY;
+        u32 tot;
+        const u32 p = block_exclusive_scan<u32>(c ? 1u : 0u, tot, scan_sm) + cnt_sm[0];
+        if (c) {
+            S.cands[p] = u;
+            S.ck[p] = r.keys[u];
+        }
+        __syncthreads();
+        if (tid == 0) cnt_sm[0] += tot;
+        __syncthreads();
+    }
+    const u32 cc = cnt_sm[0];
+    // 2. stable sort by key
+    u32 *sk = S.ck, *sv = S.cands;
+    if (block_sort_pairs(S.ck, S.cands, S.ck2, S.cands2, cc, key_bits, offs, wc, scan_sm)) {
+        sk = S.ck2;
+        sv = S.cands2;
+    }
+    // 3. weight prefix over the sorted candidates (prefix[cc] = total)
+    long long carry = 0;
+    for (u32 base = 0; base <= cc; base += OB) {
+        const u32 i = base + tid;
+        const long long v = i < cc ? (long long) g_vw(a.g, sv[i]) : 0;
+        long long tot;
+        const long long p = block_exclusive_scan<long long>(v, tot, lsm) + carry;
+        if (i <= cc) S.prefix[i] = p;
+        carry += tot;
+        __syncthreads();
+    }
+    // 4. B(x) for x = p * width, p in [0, k]
+    for (u32 pb = tid; pb <= a.k; pb += OB) {
+        const u64 x = (u64) pb * width;
+        u32 lo = 0, hi = cc;
+        while (lo < hi) {
+            const u32 mid = (lo + hi) >> 1;
+            if ((u64) sk[mid] < x) lo = mid + 1;
+            else hi = mid;
+        }
+        S.B[pb] = S.prefix[lo];
+    }
+    __syncthreads();
+    // 5. moves
+    for (u32 i = tid; i < cc; i += OB) {
+        const u32 u = sv[i];
+        const u32 o = a.map[u];
+        const long long score = S.prefix[i] - S.B[o];
+        const long long limit = (long long) a.bw[o] - a.lmax;
+        if (score < limit) {
+            const u32 s = atomicAdd(&cnt_sm[1], 1u);
+            a.moves[s] = u;
+            if (STRONG) {
+                S.mpre[s] = S.prefix[i];
+                const long long vw = g_vw(a.g, u);
+                if (score + vw >= limit) S.ea[o] = score + vw;
+            }
+        }
+    }
+    __syncthreads();
+    const u32 nm = cnt_sm[1];
+    if (!STRONG) {
+        if (tid == 0) a.st->cnt[ST_MOVES] = nm;
+        return;
+    }
+    // 6. cookie cutter
+    long long *max_v = (long long *) &a.st->sum[3];
+    cookie_block(a.bw, a.k, max_b_w, S.B, S.ea, S.es, max_v, lsm);
+    __syncthreads();
+    // 7. first slot attempt
+    for (u32 j = tid; j < nm; j += OB) {
+        const u32 u = a.moves[j];
+        if (strong_assign_one(a, u, S.mpre[j], S.ea, S.es)) S.fail[atomicAdd(&cnt_sm[2], 1u)] = u;
+    }
+    __syncthreads();
+    // 8. fallback slots in ascending vertex id
+    const u32 nf = cnt_sm[2];
+    if (nf) {
+        u32 *fk = S.fail, *fv = S.fail2;
+        // sort ids (keys) carrying themselves as values: (fail, fail2) -> sorted
+        for (u32 i = tid; i < nf; i += OB) S.fail2[i] = S.fail[i];
+        __syncthreads();
+        u32 *k1 = S.cands, *v1 = S.cands2;  // free after step 5
+        if (block_sort_pairs(S.fail, S.fail2, k1, v1, nf, bits_for_u32(n), offs, wc, scan_sm)) fk = k1;
+        __syncthreads();
+        (void) fv;
+        if (tid == 0) strong_fallback_seq(a, fk, nf, S.es, max_v);
+    }
+    if (tid == 0) a.st->cnt[ST_MOVES] = nm;
 }
 
 // ---- objectives ------------------------------------------------------------------
@@ -1360,14 +1585,22 @@ void sections_of(u32 n, u32 k, u32 &sections, u32 &width) {
     width = MAX_BUCKETS * sections;
 }
 
+// Raises the dynamic shared-memory limit of the block-tier kernels, once per
+// device (function attributes are per device; several host threads may get
+// here at once).
 void set_big_smem() {
-    static bool done = false;
-    if (done) return;
+    static std::mutex mu;
+    static std::vector<int> done;
+    int dev = 0;
+    HP_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    for (int d: done)
+        if (d == dev) return;
     const int smem = (int) (JB_SLOTS * 8);
     HP_CUDA(cudaFuncSetAttribute(k_lp_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     HP_CUDA(cudaFuncSetAttribute(k_rb_block<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     HP_CUDA(cudaFuncSetAttribute(k_rb_block<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    done = true;
+    done.push_back(dev);
 }
 
 } // namespace
@@ -1546,8 +1779,6 @@ void JetLevel::lp(u32 ratio_pct) {
         KernTimer kt(c, "k_lp_filter");
         k_lp_filter<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }
-    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
-    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
     KernTimer kt(c, "k_afterburner");
     {
         KernTimer kt1(c, "k_ab_thread");
@@ -1605,6 +1836,19 @@ void JetLevel::weak() {
     }
     ProfScope p3(c, "weak.order");
     HP_LAUNCH_CHECK();
+    if (n <= ORDER_SMALL_N) {
+        OrderScratch S{};
+        S.cands = c.balloc<u32>(n);
+        S.ck = c.balloc<u32>(n);
+        S.cands2 = c.balloc<u32>(n);
+        S.ck2 = c.balloc<u32>(n);
+        S.prefix = c.balloc<long long>((u64) n + 1);
+        S.B = c.balloc<long long>((u64) k + 1);
+        k_order_small<false><<<1, OB, 0, c.stream>>>(a, r, width, bits_for((u64) MAX_BUCKETS * k * sections + 1), S,
+                                                     max_b_w); note_launch();
+        HP_LAUNCH_CHECK();
+        return;
+    }
     // ordered candidates (ascending id), then a stable sort by mini-bucket key
     u32 *cands = c.balloc<u32>(n);
     u32 *ck = c.balloc<u32>(n);
@@ -1677,6 +1921,24 @@ void JetLevel::strong() {
     }
     ProfScope p3(c, "strong.order");
     HP_LAUNCH_CHECK();
+    if (n <= ORDER_SMALL_N) {
+        OrderScratch S{};
+        S.cands = c.balloc<u32>(n);
+        S.ck = c.balloc<u32>(n);
+        S.cands2 = c.balloc<u32>(n);
+        S.ck2 = c.balloc<u32>(n);
+        S.prefix = c.balloc<long long>((u64) n + 1);
+        S.B = c.balloc<long long>((u64) k + 1);
+        S.ea = c.balloc<long long>(k);
+        S.es = c.balloc<long long>((u64) k + 1);
+        S.mpre = c.balloc<long long>((u64) n + 1);
+        S.fail = c.balloc<u32>(n);
+        S.fail2 = c.balloc<u32>(n);
+        k_order_small<true><<<1, OB, 0, c.stream>>>(a, r, width, bits_for((u64) MAX_BUCKETS * k * sections + 2), S,
+                                                    max_b_w); note_launch();
+        HP_LAUNCH_CHECK();
+        return;
+    }
     u32 *cands = c.balloc<u32>(n);
     u32 *ck = c.balloc<u32>(n);
     device_scan<u32>(
@@ -1727,16 +1989,12 @@ void JetLevel::perform() {
     ProfScope prof(c, "jet.perform");
     JArgs a = make_args(*this);
     const u32 n = g.n;
-    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY], 0, sizeof(u32), c.stream));
-    HP_CUDA(cudaMemsetAsync(&c.d_status->cnt[ST_HEAVY2], 0, sizeof(u32), c.stream));
-    HP_CUDA(cudaMemsetAsync(&c.d_status->sum[SUM_DELTA], 0, sizeof(long long), c.stream));
-    HP_CUDA(cudaMemsetAsync(&c.d_status->sum[SUM_PERF_ENTRIES], 0, sizeof(long long), c.stream));
+    k_perform_reset<<<1, 32, 0, c.stream>>>(c.d_status); note_launch();
     {
         // labels first (new label + MOVED bit, old label in dest_part) ...
         ProfScope p2(c, "perform.apply");
         KernTimer kt(c, "k_apply");
         k_apply<<<c.grid(n, BLOCK), BLOCK, k <= APPLY_SMEM_K ? k * sizeof(s32) : 0, c.stream>>>(a); note_launch();
-        k_max_bw<<<1, 1024, 0, c.stream>>>(bw, k, &c.d_status->imax[MAX_BW]); note_launch();
     }
     {
         // ... then the exact objective change and the neighbours' cache resets
@@ -1751,8 +2009,7 @@ void JetLevel::perform() {
             KernTimer kt1(c, "k_delta_chunk");
             k_delta_chunk<<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
         }
-        k_inval_all<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-        k_unmark<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        k_inval_unmark<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }
     HP_LAUNCH_CHECK();
 }
