@@ -4,13 +4,24 @@
 #include "coarsen.cuh"
 #include "prims.cuh"
 
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
 namespace hp {
 namespace {
 
+// Reads of vcmap: plain in kernels that do not write it, L2-coherent (no L1)
+// in the fused matching loop, where other blocks write it between phases.
+template<bool COH>
+__device__ __forceinline__ u32 ld_vc(const u32 *p) {
+    return COH ? __ldcg(p) : *p;
+}
+
 // Argmax over the eligible neighbours of u of (edge weight, xorshift(v + r)),
 // r = xorshift(u ^ seed): pick_neighbor_flat two_hop_matching.h:102-141.
-template<bool INITIAL>
-__device__ __forceinline__ u32 pick_thread(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed) {
+template<bool INITIAL, bool COH = false>
+__device__ __forceinline__ u32 pick_thread(const DGraph &g, const u32 *vcmap, u32 u, u32 seed) {
     const u32 r = xorshift32(u ^ seed);
     const u64 beg = g.rowptr[u];
     const u32 len = g.rowlen[u];
@@ -18,7 +29,7 @@ __device__ __forceinline__ u32 pick_thread(const DGraph &g, const u32 *__restric
     s32 maxw = 0;
     for (u32 t = 0; t < len; ++t) {
         const u32 v = g.adj[beg + t];
-        if (!INITIAL && vcmap[v] != SENTINEL) continue;
+        if (!INITIAL && ld_vc<COH>(&vcmap[v]) != SENTINEL) continue;
         if (g.ew) {
             const s32 w = g.ew[beg + t];
             if (maxw < w) {
@@ -48,16 +59,16 @@ struct PickLocal {
     u32 h;
 };
 
-template<bool INITIAL>
-__device__ __forceinline__ PickLocal pick_local(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed,
-                                                u32 tid, u32 nthreads) {
+template<bool INITIAL, bool COH = false>
+__device__ __forceinline__ PickLocal pick_local(const DGraph &g, const u32 *vcmap, u32 u, u32 seed, u32 tid,
+                                                u32 nthreads) {
     const u32 r = xorshift32(u ^ seed);
     const u64 beg = g.rowptr[u];
     const u32 len = g.rowlen[u];
     PickLocal p{false, 0, 0, SENTINEL};
     for (u32 t = tid; t < len; t += nthreads) {
         const u32 v = g.adj[beg + t];
-        if (!INITIAL && vcmap[v] != SENTINEL) continue;
+        if (!INITIAL && ld_vc<COH>(&vcmap[v]) != SENTINEL) continue;
         const s32 w = g.ew ? g.ew[beg + t] : 0;
         const u32 tb = xorshift32(v + r);
         if (!p.found || w > p.w || (w == p.w && tb >= p.tb)) p = PickLocal{true, w, tb, v};
@@ -75,16 +86,15 @@ __device__ __forceinline__ PickLocal pick_reduce_warp(PickLocal p) {
     return PickLocal{true, wbest, tbest, __shfl_sync(FULL, p.h, __ffs(win) - 1)};
 }
 
-template<bool INITIAL>
-__device__ __forceinline__ u32 pick_warp(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed) {
-    return pick_reduce_warp(pick_local<INITIAL>(g, vcmap, u, seed, lane_id(), 32)).h;
+template<bool INITIAL, bool COH = false>
+__device__ __forceinline__ u32 pick_warp(const DGraph &g, const u32 *vcmap, u32 u, u32 seed) {
+    return pick_reduce_warp(pick_local<INITIAL, COH>(g, vcmap, u, seed, lane_id(), 32)).h;
 }
 
 // Block argmax: warp winners go through shared memory to thread 0.
-template<bool INITIAL>
-__device__ __forceinline__ u32 pick_block(const DGraph &g, const u32 *__restrict__ vcmap, u32 u, u32 seed,
-                                          PickLocal *sm) {
-    PickLocal p = pick_reduce_warp(pick_local<INITIAL>(g, vcmap, u, seed, threadIdx.x, blockDim.x));
+template<bool INITIAL, bool COH = false>
+__device__ __forceinline__ u32 pick_block(const DGraph &g, const u32 *vcmap, u32 u, u32 seed, PickLocal *sm) {
+    PickLocal p = pick_reduce_warp(pick_local<INITIAL, COH>(g, vcmap, u, seed, threadIdx.x, blockDim.x));
     if (lane_id() == 0) sm[warp_in_block()] = p;
     __syncthreads();
     u32 h = SENTINEL;
@@ -232,6 +242,119 @@ __global__ void k_repick(DGraph g, const u32 *list, u32 cnt, const u32 *vcmap, u
     }
 }
 
+// The whole matching loop of one level in one cooperative launch (grid-wide
+// barriers between the phases the per-phase kernels above run separately):
+// per round the receiver marks, four commit sub-rounds of claim and resolve,
+// the re-pick (thread, warp and block tiers) and the compaction of the
+// still-unmatched list. Data written by other blocks is read through L2
+// (__ldcg), never from L1. The list order does not affect the result (claims
+// keep the smallest proposer, picks are per vertex), so the compaction
+// appends atomically. ctr: [0] next list length, [1] warp-tier picks, [2]
+// block-tier picks, [3] rounds run, [4] error.
+constexpr u32 MATCH_MAX_ROUNDS = 100000;
+constexpr u32 MATCH_COOP_MAX_N = 1u << 17;  // levels up to this many vertices ...
+constexpr u64 MATCH_COOP_MAX_M = 1u << 21;  // ... and CSR entries use the fused loop
+
+__global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap, u32 *hn, u32 *list, u32 *list2,
+                                                           u32 cnt, unsigned long long *claim, u32 *heavy, u32 *huge,
+                                                           u32 *ctr, u32 seed) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ PickLocal sm[32];
+    const u64 gtid = (u64) blockIdx.x * blockDim.x + threadIdx.x;
+    const u64 gsize = (u64) gridDim.x * blockDim.x;
+    const u32 warps = (u32) (gsize >> 5);
+    const u32 gwarp = (u32) (gtid >> 5);
+    u32 epoch = 0;
+    for (u32 round = 0; cnt > 0; ++round) {
+        if (round >= MATCH_MAX_ROUNDS) {
+            if (gtid == 0) ctr[4] = 1;
+            break;
+        }
+        const u32 round_seed = seed ^ (round * 0x9e3779b1u);
+        if (gtid == 0) {
+            ctr[0] = 0;
+            ctr[1] = 0;
+            ctr[2] = 0;
+        }
+        // commit_p1: receivers of sub-round 0
+        for (u64 i = gtid; i < cnt; i += gsize) {
+            const u32 u = list[i];
+            const u32 v = __ldcg(&hn[u]);
+            if (v == SENTINEL || __ldcg(&vcmap[u]) != SENTINEL) continue;
+            if (!commit_cond(u, v, 0)) vcmap[u] = SENTINEL - 1;
+        }
+        grid.sync();
+        for (u32 r = 0; r < 4; ++r) {
+            ++epoch;
+            const u32 tag = 0xFFFFFFFFu - epoch;
+            for (u64 i = gtid; i < cnt; i += gsize) {
+                const u32 u = list[i];
+                const u32 v = __ldcg(&hn[u]);
+                if (v == SENTINEL || __ldcg(&vcmap[u]) != SENTINEL) continue;
+                if (__ldcg(&vcmap[v]) == SENTINEL - 1) atomicMin(&claim[v], ((unsigned long long) tag << 32) | u);
+            }
+            grid.sync();
+            const int next_r = r < 3 ? (int) r + 1 : -1;
+            for (u64 i = gtid; i < cnt; i += gsize) {
+                const u32 u = list[i];
+                u32 st = __ldcg(&vcmap[u]);
+                const u32 v = __ldcg(&hn[u]);
+                if (st == SENTINEL - 1) {
+                    const unsigned long long c = __ldcg(&claim[u]);
+                    st = (u32) (c >> 32) == tag ? (u < (u32) c ? u : (u32) c) : SENTINEL;
+                } else if (st == SENTINEL && v != SENTINEL) {
+                    const unsigned long long c = __ldcg(&claim[v]);
+                    if ((u32) (c >> 32) == tag && (u32) c == u) st = u < v ? u : v;
+                }
+                if (next_r >= 0 && st == SENTINEL && v != SENTINEL && !commit_cond(u, v, (u32) next_r))
+                    st = SENTINEL - 1;
+                vcmap[u] = st;
+            }
+            grid.sync();
+        }
+        // re-pick for vertices whose target got matched
+        for (u64 base = (u64) blockIdx.x * blockDim.x; base < cnt; base += gsize) {
+            const u64 i = base + threadIdx.x;
+            int tier = 0;
+            u32 u = 0;
+            if (i < cnt) {
+                u = list[i];
+                const u32 h = __ldcg(&hn[u]);
+                if (__ldcg(&vcmap[u]) == SENTINEL && h != SENTINEL && __ldcg(&vcmap[h]) != SENTINEL) {
+                    tier = pick_tier(g.rowlen[u]);
+                    if (tier == 0) hn[u] = pick_thread<false, true>(g, vcmap, u, round_seed);
+                }
+            }
+            append_tier(tier, u, heavy, &ctr[1], huge, &ctr[2]);
+        }
+        grid.sync();
+        const u32 nh = __ldcg(&ctr[1]), ng = __ldcg(&ctr[2]);
+        for (u32 i = gwarp; i < nh; i += warps) {
+            const u32 u = heavy[i];
+            const u32 h = pick_warp<false, true>(g, vcmap, u, round_seed);
+            if (lane_id() == 0) hn[u] = h;
+        }
+        for (u32 i = blockIdx.x; i < ng; i += gridDim.x) {
+            const u32 u = huge[i];
+            const u32 h = pick_block<false, true>(g, vcmap, u, round_seed, sm);
+            if (threadIdx.x == 0) hn[u] = h;
+        }
+        grid.sync();
+        // still unmatched with a target: next round's list
+        for (u64 i = gtid; i < cnt; i += gsize) {
+            const u32 u = list[i];
+            if (__ldcg(&vcmap[u]) == SENTINEL && __ldcg(&hn[u]) != SENTINEL) list2[atomicAdd(&ctr[0], 1u)] = u;
+        }
+        grid.sync();
+        cnt = __ldcg(&ctr[0]);
+        u32 *t = list;
+        list = list2;
+        list2 = t;
+        if (gtid == 0) ctr[3] = round + 1;
+        grid.sync();  // every thread has read ctr[0] before the next round clears it
+    }
+}
+
 __global__ void k_count_unmapped(const u32 *vcmap, u32 n, u32 *out) {
     u32 c = 0;
     for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) c += vcmap[u] == SENTINEL;
@@ -368,34 +491,60 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
     device_iota(ctx, list, n);
     HP_LAUNCH_CHECK();
 
-    u32 cnt = n;
-    u32 round = 0, epoch = 0;
-    while (cnt > 0) {
-        const u32 round_seed = seed ^ (round * 0x9e3779b1u);
-        const u32 grid = ctx.grid(cnt, BLOCK);
-        k_mark<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, 0); note_launch();
-        for (u32 r = 0; r < 4; ++r) {
-            ++epoch;
-            const u32 tag = 0xFFFFFFFFu - epoch;
-            k_claim<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag); note_launch();
-            k_resolve<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag, r < 3 ? (int) r + 1 : -1); note_launch();
+    // the round loop: on small levels (launch and synchronisation cost
+    // dominates) one cooperative launch, else one launch per phase with a
+    // host read per round (large levels need more threads than fit at once)
+    int per_sm = 0;
+    if (n <= MATCH_COOP_MAX_N && g.m <= MATCH_COOP_MAX_M)
+        HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_loop, PICK_BLOCK, 0));
+    if (per_sm > 0) {
+        u32 *ctr = &ctx.d_status->cnt[8];  // 5 words, cleared below
+        HP_CUDA(cudaMemsetAsync(ctr, 0, 5 * sizeof(u32), ctx.stream));
+        const u32 want = (u32) std::max<u64>(1, ((u64) n + PICK_BLOCK - 1) / PICK_BLOCK);
+        const u32 grid = std::min<u32>(want, (u32) (per_sm * ctx.sm_count));
+        DGraph gg = g;
+        u32 *pl = list, *pl2 = list2;
+        u32 cnt0 = n;
+        u32 sd = seed;
+        void *args[] = {&gg, &vcmap, &hn, &pl, &pl2, &cnt0, &claim, &heavy, &huge, &ctr, &sd};
+        HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_match_loop, dim3(grid), dim3(PICK_BLOCK), args, 0,
+                                            ctx.stream));
+        note_launch();
+        if (ctx.read_status().cnt[12]) throw HpError{HP_ERR_DEVICE, "matching did not converge"};
+    } else {
+        u32 cnt = n;
+        u32 round = 0, epoch = 0;
+        while (cnt > 0) {
+            const u32 round_seed = seed ^ (round * 0x9e3779b1u);
+            const u32 grid = ctx.grid(cnt, BLOCK);
+            k_mark<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, 0); note_launch();
+            for (u32 r = 0; r < 4; ++r) {
+                ++epoch;
+                const u32 tag = 0xFFFFFFFFu - epoch;
+                k_claim<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag); note_launch();
+                k_resolve<<<grid, BLOCK, 0, ctx.stream>>>(list, cnt, hn, vcmap, claim, tag, r < 3 ? (int) r + 1 : -1);
+                note_launch();
+            }
+            ctx.zero_counters();
+            k_repick<<<grid, BLOCK, 0, ctx.stream>>>(g, list, cnt, vcmap, hn, round_seed, heavy, heavy_cnt, huge,
+                                                     huge_cnt); note_launch();
+            k_pick_heavy<false><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, heavy, heavy_cnt);
+            note_launch();
+            k_pick_huge<false><<<hgrid, PICK_BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, huge, huge_cnt);
+            note_launch();
+            HP_LAUNCH_CHECK();
+            const u32 *l = list;
+            device_select(
+                ctx, cnt, [=] __device__(u64 i) -> bool {
+                    const u32 u = l[i];
+                    return vcmap[u] == SENTINEL && hn[u] != SENTINEL;
+                },
+                [=] __device__(u64 i) -> u32 { return l[i]; }, list2, &ctx.d_status->cnt[0]);
+            cnt = ctx.read_status().cnt[0];
+            std::swap(list, list2);
+            ++round;
+            if (round > 100000) throw HpError{HP_ERR_DEVICE, "matching did not converge"};
         }
-        ctx.zero_counters();
-        k_repick<<<grid, BLOCK, 0, ctx.stream>>>(g, list, cnt, vcmap, hn, round_seed, heavy, heavy_cnt, huge, huge_cnt); note_launch();
-        k_pick_heavy<false><<<wgrid, BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, heavy, heavy_cnt); note_launch();
-        k_pick_huge<false><<<hgrid, PICK_BLOCK, 0, ctx.stream>>>(g, vcmap, hn, round_seed, huge, huge_cnt); note_launch();
-        HP_LAUNCH_CHECK();
-        const u32 *l = list;
-        device_select(
-            ctx, cnt, [=] __device__(u64 i) -> bool {
-                const u32 u = l[i];
-                return vcmap[u] == SENTINEL && hn[u] != SENTINEL;
-            },
-            [=] __device__(u64 i) -> u32 { return l[i]; }, list2, &ctx.d_status->cnt[0]);
-        cnt = ctx.read_status().cnt[0];
-        std::swap(list, list2);
-        ++round;
-        if (round > 100000) throw HpError{HP_ERR_DEVICE, "matching did not converge"};
     }
 
     u32 unmapped = count_unmapped(ctx, vcmap, n);
