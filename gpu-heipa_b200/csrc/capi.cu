@@ -626,6 +626,21 @@ int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t
     return HP_OK;
 }
 
+int hp_tune(hp_ctx *ctx, const char *name, int64_t value) {
+    if (!ctx || !name || value < 0) return HP_ERR_ARG;
+    hp::Tunables &t = ctx->c.tune;
+    const std::string nm(name);
+    if (nm == "jet_graph_max_m") t.jet_graph_max_m = (uint64_t) value;
+    else if (nm == "order_small_n") t.order_small_n = (uint32_t) std::min<int64_t>(value, 0xFFFFFFFFll);
+    else if (nm == "match_coop_max_n") t.match_coop_max_n = (uint32_t) std::min<int64_t>(value, 0xFFFFFFFFll);
+    else if (nm == "match_coop_max_m") t.match_coop_max_m = (uint64_t) value;
+    else {
+        ctx->c.last_error = "unknown tunable " + nm;
+        return HP_ERR_ARG;
+    }
+    return HP_OK;
+}
+
 int hp_instrument(hp_ctx *ctx, int enable) {
     if (!ctx) return HP_ERR_ARG;
     return guarded(ctx, [&] {

@@ -189,6 +189,7 @@ Ctx &Ctx::worker(size_t i) {
         }
         workers.push_back(std::move(w));
     }
+    workers[i]->tune = tune;
     return *workers[i];
 }
 

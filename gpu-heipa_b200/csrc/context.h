@@ -123,8 +123,18 @@ struct PhaseProf {
     }
 };
 
+// Size thresholds that choose between equivalent implementations (results
+// are identical either way; only the launch structure differs).
+struct Tunables {
+    u64 jet_graph_max_m = 1ull << 24;  // Jet iterations replayed as CUDA graphs up to this many entries
+    u32 order_small_n = 4096;          // single-block rebalance ordering up to this many vertices
+    u32 match_coop_max_n = 1u << 17;   // cooperative matching loop up to this many vertices ...
+    u64 match_coop_max_m = 1ull << 21; // ... and entries
+};
+
 struct Ctx {
     int device = 0;
+    Tunables tune;
     int sm_count = NUM_SMS_HINT;
     cudaStream_t stream = nullptr;
     Arena arena;

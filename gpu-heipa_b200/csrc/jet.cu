@@ -1836,7 +1836,7 @@ void JetLevel::weak() {
     }
     ProfScope p3(c, "weak.order");
     HP_LAUNCH_CHECK();
-    if (n <= ORDER_SMALL_N) {
+    if (n <= std::min<u32>(c.tune.order_small_n, ORDER_SMALL_N)) {
         OrderScratch S{};
         S.cands = c.balloc<u32>(n);
         S.ck = c.balloc<u32>(n);
@@ -1921,7 +1921,7 @@ void JetLevel::strong() {
     }
     ProfScope p3(c, "strong.order");
     HP_LAUNCH_CHECK();
-    if (n <= ORDER_SMALL_N) {
+    if (n <= std::min<u32>(c.tune.order_small_n, ORDER_SMALL_N)) {
         OrderScratch S{};
         S.cands = c.balloc<u32>(n);
         S.ck = c.balloc<u32>(n);
@@ -2072,7 +2072,7 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
     // one filter ratio per level (or none for the mapping objective): a
     // recomputed gain then equals a still-valid cached one
     L.cache_pure = promap || !ultra;
-    L.graphs = g.m <= JET_GRAPH_MAX_M && !ctx.prof.enabled;
+    L.graphs = g.m <= ctx.tune.jet_graph_max_m && !ctx.prof.enabled;
     s64 best_obj = obj;
     s32 best_max = maxw;
     std::vector<u32> ratios;

@@ -114,9 +114,8 @@ private:
     std::vector<StepGraph> step_graphs;
 };
 
-// Levels up to this many CSR entries replay their Jet iterations as CUDA
-// graphs (launch and synchronisation cost dominates there).
-constexpr u64 JET_GRAPH_MAX_M = 1ull << 24;
+// Levels up to Tunables::jet_graph_max_m CSR entries replay their Jet
+// iterations as CUDA graphs (launch and synchronisation cost dominates there).
 
 // Status word slots used by Jet.
 constexpr int ST_MOVES = 3;

@@ -252,8 +252,9 @@ __global__ void k_repick(DGraph g, const u32 *list, u32 cnt, const u32 *vcmap, u
 // appends atomically. ctr: [0] next list length, [1] warp-tier picks, [2]
 // block-tier picks, [3] rounds run, [4] error.
 constexpr u32 MATCH_MAX_ROUNDS = 100000;
-constexpr u32 MATCH_COOP_MAX_N = 1u << 17;  // levels up to this many vertices ...
-constexpr u64 MATCH_COOP_MAX_M = 1u << 21;  // ... and CSR entries use the fused loop
+// upper bound of Tunables::match_coop_max_n (the grid of the fused loop holds
+// every list entry in a few grid-stride passes)
+constexpr u32 MATCH_COOP_MAX_N = 1u << 20;
 
 __global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap, u32 *hn, u32 *list, u32 *list2,
                                                            u32 cnt, unsigned long long *claim, u32 *heavy, u32 *huge,
@@ -495,7 +496,7 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
     // dominates) one cooperative launch, else one launch per phase with a
     // host read per round (large levels need more threads than fit at once)
     int per_sm = 0;
-    if (n <= MATCH_COOP_MAX_N && g.m <= MATCH_COOP_MAX_M)
+    if (n <= std::min<u32>(ctx.tune.match_coop_max_n, MATCH_COOP_MAX_N) && g.m <= ctx.tune.match_coop_max_m)
         HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_loop, PICK_BLOCK, 0));
     if (per_sm > 0) {
         u32 *ctr = &ctx.d_status->cnt[8];  // 5 words, cleared below

@@ -67,6 +67,7 @@ _SIG = {
     "hp_last_solve_stats": (_int, [_vp, _vp, _vp, _vp, _vp]),
     "hp_last_solve_maxw": (_int, [_vp, _vp, _vp]),
     "hp_last_solve_level": (_int, [_vp, _u32, _vp, _vp]),
+    "hp_tune": (_int, [_vp, ctypes.c_char_p, _i64]),
     "hp_instrument": (_int, [_vp, _int]),
     "hp_kernel_timing": (_int, [_vp, ctypes.c_char_p, _vp, _vp, _vp]),
     "hp_kernel_log": (_int, [_vp, _u64, ctypes.c_char_p, ctypes.c_size_t, _vp, _vp]),
@@ -514,6 +515,10 @@ class Context:
             out[buf.value.decode()] = (ms.value, cnt.value)
             i += 1
         return out
+
+    def tune(self, name, value):
+        """hp_tune: set a size threshold between equivalent implementations."""
+        self._check(_L.hp_tune(self.h, name.encode(), int(value)))
 
     def instrument(self, enable=True):
         self._check(_L.hp_instrument(self.h, int(enable)))

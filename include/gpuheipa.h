@@ -174,6 +174,15 @@ int hp_last_solve_maxw(const hp_ctx *ctx, int32_t *initial_maxw, int32_t *final_
  * per-level "n m" lines of solver.h:358; HP_ERR_ARG past the last level. */
 int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t *m);
 
+/* Sets a size threshold that chooses between equivalent implementations
+ * (results are identical; only the launch structure changes): "jet_graph_max_m"
+ * (levels up to this many CSR entries replay Jet iterations as CUDA graphs;
+ * 0 = never), "order_small_n" (single-block rebalance ordering up to this many
+ * vertices, at most 4096; 0 = never), "match_coop_max_n" / "match_coop_max_m"
+ * (one cooperative launch for the matching loop of levels up to these sizes;
+ * 0 = never). Unknown names return HP_ERR_ARG. No counterpart in the reference. */
+int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
+
 /* Enables CUDA-event timing of the contraction and Jet-gain kernels on ctx;
  * hp_kernel_timing reports launches, total ms and algorithmic bytes. */
 int hp_instrument(hp_ctx *ctx, int enable);

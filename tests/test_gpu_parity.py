@@ -268,3 +268,45 @@ def test_invalid_inputs_rejected(ctx):
     with pytest.raises(H.HeiPaError):
         ctx.upload(zero_w)
     assert "invalid graph" in ctx.last_error()
+
+
+def test_direct_launch_paths_equal(ctx):
+    # Small test graphs take the CUDA-graph, single-block-ordering and
+    # cooperative-matching paths; force the per-kernel launch paths of large
+    # levels and require the same results.
+    g = H.Graph.rmat(14, 16, seed=3)
+    m = H.Graph.rgg3d(20000, 14.0, 1, 100, seed=8, explicit_vw=True)
+    want_p, want_c = ctx.partition(g, 64, 0.03, "default", 7)
+    want_m, want_j = ctx.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, "HM", 3)
+    c2 = H.Context(0, 2 << 30)
+    try:
+        for name in ("jet_graph_max_m", "order_small_n", "match_coop_max_n", "match_coop_max_m"):
+            c2.tune(name, 0)
+        part, cut = c2.partition(g, 64, 0.03, "default", 7)
+        assert cut == want_c
+        np.testing.assert_array_equal(part, want_p)
+        mp, J = c2.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, "HM", 3)
+        assert J == want_j
+        np.testing.assert_array_equal(mp, want_m)
+        opart, ocut = O.partition(to_oracle(g), 64, 0.03, False, 7)
+        assert ocut == cut
+        with pytest.raises(H.HeiPaError):
+            c2.tune("no_such_threshold", 1)
+    finally:
+        c2.close()
+
+
+def test_arena_exhaustion_is_an_error():
+    small = H.Context(0, 64 << 20)
+    try:
+        g = H.Graph.rmat(16, 16, seed=1)
+        with pytest.raises(H.HeiPaError) as e:
+            small.partition(g, 8)
+        assert e.value.code == 3
+        # the context stays usable for a graph that fits
+        p, c = small.partition(H.Graph.grid(32, 32), 4, seed=1)
+        op, oc = O.partition(to_oracle(H.Graph.grid(32, 32)), 4, 0.03, False, 1)
+        np.testing.assert_array_equal(p, op)
+        assert c == oc
+    finally:
+        small.close()
