@@ -69,3 +69,21 @@ def test_server_rejects_oversized_request():
 def test_server_without_device_is_an_error():
     with pytest.raises(H.HeiPaError):
         H.Server(0, 1 << 20, 2)
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_results(ctx):
+    import autotune
+    graphs = [H.Graph.grid(60, 60), H.Graph.rgg3d(8000, 10.0, 1, 10, seed=2)]
+    ks = [8, 16]
+    before = [ctx.partition(g, k, 0.03, "default", 1) for g, k in zip(graphs, ks)]
+    small = {"jet_graph_max_m": [0, 1 << 24], "order_small_n": [0, 4096], "match_coop_max_n": [0, 1 << 17],
+             "match_coop_max_m": [1 << 21]}
+    best = autotune.tune(ctx, graphs, ks, candidates=small, repeats=1)
+    assert set(best) == set(autotune.DEFAULTS)
+    after = [ctx.partition(g, k, 0.03, "default", 1) for g, k in zip(graphs, ks)]
+    for (p0, c0), (p1, c1) in zip(before, after):
+        np.testing.assert_array_equal(p0, p1)
+        assert c0 == c1
+    for name, v in autotune.DEFAULTS.items():  # leave the session context as it was
+        ctx.tune(name, v)
