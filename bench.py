@@ -51,6 +51,8 @@ RGG_DESC = ("3D RGG {n} points, mean degree 14, edge weights U[1,100], explicit 
 WORKLOADS = {
     "rmat22": dict(kind="rmat", scale=22, task="partition", k=64, desc=RMAT_DESC.format(s=22),
                    sample=dict(kind="rmat", scale=18)),
+    "rmat20": dict(kind="rmat", scale=20, task="partition", k=64, desc=RMAT_DESC.format(s=20) + " (profiling case)",
+                   sample=dict(kind="rmat", scale=18)),
     "rmat18": dict(kind="rmat", scale=18, task="partition", k=64, desc=RMAT_DESC.format(s=18) + " (profiling case)",
                    sample=dict(kind="rmat", scale=18)),
     "grid256": dict(kind="grid", w=256, h=256, task="partition", k=16,
@@ -424,6 +426,9 @@ def run_ours(args, world, rank, local):
     g = make_graph(H, wl, args.seed)
     edges = g.m // 2
     ctx = H.Context(local, H.arena_estimate(g.n, g.m, g.ew is not None, g.vw is not None))
+    for t in args.tune:
+        name, value = t.split("=")
+        ctx.tune(name, int(value))
     dg = ctx.upload(g)
     part = np.empty(g.n, np.uint32)
     for _ in range(args.warmup):
@@ -540,6 +545,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--kernel-timers", action="store_true", help="print every kernel timer to stderr")
     ap.add_argument("--workers", type=int, default=8, help="concurrent requests (batch / served workloads)")
+    ap.add_argument("--tune", action="append", default=[], metavar="NAME=VALUE",
+                    help="launch-structure threshold (hp_tune), e.g. jet_graph_max_m=0 for profiling runs")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if world > 1:

@@ -154,7 +154,13 @@ __device__ __forceinline__ void set_error(u32 *err, u32 bits) { atomicOr(err, bi
 // Number of kernels this process has launched (every launch site calls
 // note_launch()).
 extern std::atomic<unsigned long long> g_kernel_launches;
-inline void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+// Launches of the calling host thread (graph capture counts its own launches
+// with it while other threads may launch concurrently).
+extern thread_local unsigned long long t_kernel_launches;
+inline void note_launch() {
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+    ++t_kernel_launches;
+}
 
 // Grid sizing: a multiple of the SM count, capped by the work.
 inline u32 grid_for(u64 items, u32 per_block, u32 max_blocks = NUM_SMS_HINT * 16) {

@@ -5,6 +5,7 @@
 namespace hp {
 
 std::atomic<unsigned long long> g_kernel_launches{0};
+thread_local unsigned long long t_kernel_launches = 0;
 
 static constexpr size_t ALIGN = 256;
 

@@ -2034,13 +2034,18 @@ void JetLevel::run_step(int kind, u32 ratio_pct) {
         return;
     }
     cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels = 0;
     for (const StepGraph &sg: step_graphs)
-        if (sg.kind == kind && sg.ratio == ratio_pct) exec = sg.exec;
+        if (sg.kind == kind && sg.ratio == ratio_pct) {
+            exec = sg.exec;
+            kernels = sg.kernels;
+        }
     if (!exec) {
         // Scratch allocated inside the step is released when it returns and
         // nothing else allocates while the level's iterations run, so the
         // addresses baked into the graph stay valid for every replay.
         cudaGraph_t graph = nullptr;
+        const unsigned long long before = t_kernel_launches;
         HP_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
         c.instr.capturing = c.prof.capturing = true;
         try {
@@ -2053,12 +2058,17 @@ void JetLevel::run_step(int kind, u32 ratio_pct) {
         }
         c.instr.capturing = c.prof.capturing = false;
         HP_CUDA(cudaStreamEndCapture(c.stream, &graph));
+        // the capture records launches without running them: count them
+        // on every replay instead
+        kernels = t_kernel_launches - before;
+        g_kernel_launches -= kernels;
         const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         HP_CUDA(e);
-        step_graphs.push_back(StepGraph{kind, ratio_pct, exec});
+        step_graphs.push_back(StepGraph{kind, ratio_pct, exec, kernels});
     }
     HP_CUDA(cudaGraphLaunch(exec, c.stream));
+    g_kernel_launches += kernels;
     c.sync();
 }
 

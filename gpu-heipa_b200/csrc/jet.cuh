@@ -110,6 +110,7 @@ private:
         int kind;
         u32 ratio;
         cudaGraphExec_t exec;
+        unsigned long long kernels;  // kernel launches in the captured sequence
     };
     std::vector<StepGraph> step_graphs;
 };
