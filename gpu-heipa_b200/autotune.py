@@ -18,11 +18,11 @@ import numpy as np
 
 CANDIDATES = {
     "jet_graph_max_m": [0, 1 << 20, 1 << 22, 1 << 24, 1 << 26],
-    "order_small_n": [0, 1024, 2048, 4096],
+    "order_small_n": [0, 4096, 16384, 65536],
     "match_coop_max_n": [0, 1 << 15, 1 << 17, 1 << 19],
     "match_coop_max_m": [0, 1 << 19, 1 << 21, 1 << 23],
 }
-DEFAULTS = {"jet_graph_max_m": 1 << 24, "order_small_n": 4096, "match_coop_max_n": 1 << 17,
+DEFAULTS = {"jet_graph_max_m": 1 << 24, "order_small_n": 16384, "match_coop_max_n": 1 << 17,
             "match_coop_max_m": 1 << 21}
 
 

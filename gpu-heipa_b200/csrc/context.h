@@ -127,7 +127,7 @@ struct PhaseProf {
 // are identical either way; only the launch structure differs).
 struct Tunables {
     u64 jet_graph_max_m = 1ull << 24;  // Jet iterations replayed as CUDA graphs up to this many entries
-    u32 order_small_n = 4096;          // single-block rebalance ordering up to this many vertices
+    u32 order_small_n = 16384;         // single-block rebalance ordering up to this many vertices
     u32 match_coop_max_n = 1u << 17;   // cooperative matching loop up to this many vertices ...
     u64 match_coop_max_m = 1ull << 21; // ... and entries
 };

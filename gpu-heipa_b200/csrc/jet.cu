@@ -1344,13 +1344,13 @@ __device__ __forceinline__ int bits_for_u32(u32 x) { return x ? 32 - __clz(x) : 
 
 // ---- rebalance ordering of small levels in one block -------------------------------
 
-// Levels of at most ORDER_SMALL_N vertices run the whole ordering of a
+// Levels of at most Tunables::order_small_n vertices run the whole ordering of a
 // rebalance step (candidate compaction, stable sort by mini-bucket key,
 // weight prefix, bucket bounds, move selection and, for strong rebalancing,
 // the cookie cutter and slot assignment) in one 1024-thread block instead of
 // ~25 small launches. The block reads and writes its own arrays only, with a
 // __syncthreads() between phases.
-constexpr u32 ORDER_SMALL_N = 4096;
+constexpr u32 ORDER_SMALL_N = 1u << 16;  // upper bound of Tunables::order_small_n
 constexpr int OB = 1024;
 
 struct OrderScratch {

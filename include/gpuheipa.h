@@ -178,7 +178,7 @@ int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t
  * (results are identical; only the launch structure changes): "jet_graph_max_m"
  * (levels up to this many CSR entries replay Jet iterations as CUDA graphs;
  * 0 = never), "order_small_n" (single-block rebalance ordering up to this many
- * vertices, at most 4096; 0 = never), "match_coop_max_n" / "match_coop_max_m"
+ * vertices, at most 65536; 0 = never), "match_coop_max_n" / "match_coop_max_m"
  * (one cooperative launch for the matching loop of levels up to these sizes;
  * 0 = never). Unknown names return HP_ERR_ARG. No counterpart in the reference. */
 int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
