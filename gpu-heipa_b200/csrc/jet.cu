@@ -241,30 +241,30 @@ struct TRow {
     s32 c[JT];
 };
 
+// Connectivity row of a vertex of at most JT entries, in registers. All
+// entries are loaded first and their labels gathered together (JT independent
+// loads in flight instead of a chain of JT), then equal blocks are merged into
+// their first occurrence. Labels are not written by the kernels that call
+// this, so they are read through the non-coherent path.
 __device__ __forceinline__ void trow_build(const JArgs &a, u32 u, TRow &r) {
+    const u64 beg = __ldg(&a.g.rowptr[u]);
+    const u32 len = __ldg(&a.g.rowlen[u]);
 #pragma unroll
     for (int s = 0; s < (int) JT; ++s) {
-        r.b[s] = EMPTY;
-        r.c[s] = 0;
+        r.b[s] = (u32) s < len ? __ldg(&a.g.adj[beg + s]) : EMPTY;
+        r.c[s] = (u32) s < len ? g_ew(a.g, beg + s) : 0;
     }
-    const u64 beg = a.g.rowptr[u];
-    const u32 len = a.g.rowlen[u];
-    for (u32 t = 0; t < len; ++t) {
-        const u32 b = a.map[a.g.adj[beg + t]];
-        const s32 w = g_ew(a.g, beg + t);
-        bool done = false;
 #pragma unroll
-        for (int s = 0; s < (int) JT; ++s)
-            if (!done && r.b[s] == b) {
-                r.c[s] = wadd(r.c[s], w);
-                done = true;
-            }
+    for (int s = 0; s < (int) JT; ++s)
+        if (r.b[s] != EMPTY) r.b[s] = __ldg(&a.map[r.b[s]]);
 #pragma unroll
-        for (int s = 0; s < (int) JT; ++s)
-            if (!done && r.b[s] == EMPTY) {
-                r.b[s] = b;
-                r.c[s] = w;
-                done = true;
+    for (int s = 1; s < (int) JT; ++s) {
+#pragma unroll
+        for (int t = 0; t < s; ++t)
+            if (r.b[s] != EMPTY && r.b[t] == r.b[s]) {
+                r.c[t] = wadd(r.c[t], r.c[s]);
+                r.b[s] = EMPTY;
+                r.c[s] = 0;
             }
     }
 }
