@@ -25,13 +25,28 @@ __device__ __forceinline__ u32 pick_thread(const DGraph &g, const u32 *vcmap, u3
     const u32 r = xorshift32(u ^ seed);
     const u64 beg = g.rowptr[u];
     const u32 len = g.rowlen[u];
+    if (len > THREAD_DEG_MAX) return SENTINEL;  // callers use this for short rows only
+    // rows of at most THREAD_DEG_MAX entries: load the entries, gather their
+    // match state together, then take the argmax in entry order
+    u32 vs[THREAD_DEG_MAX];
+    s32 ws[THREAD_DEG_MAX];
+    bool ok[THREAD_DEG_MAX];
+#pragma unroll
+    for (int t = 0; t < (int) THREAD_DEG_MAX; ++t) {
+        vs[t] = (u32) t < len ? g.adj[beg + t] : SENTINEL;
+        ws[t] = ((u32) t < len && g.ew) ? g.ew[beg + t] : 0;
+    }
+#pragma unroll
+    for (int t = 0; t < (int) THREAD_DEG_MAX; ++t)
+        ok[t] = vs[t] != SENTINEL && (INITIAL || ld_vc<COH>(&vcmap[vs[t]]) == SENTINEL);
     u32 h = SENTINEL, tbb = 0;
     s32 maxw = 0;
-    for (u32 t = 0; t < len; ++t) {
-        const u32 v = g.adj[beg + t];
-        if (!INITIAL && ld_vc<COH>(&vcmap[v]) != SENTINEL) continue;
+#pragma unroll
+    for (int t = 0; t < (int) THREAD_DEG_MAX; ++t) {
+        if (!ok[t]) continue;
+        const u32 v = vs[t];
         if (g.ew) {
-            const s32 w = g.ew[beg + t];
+            const s32 w = ws[t];
             if (maxw < w) {
                 maxw = w;
                 h = v;
