@@ -253,3 +253,7 @@ def gain_bucket(gx, vwgt):
 
 def gain_bucket_float(gx, vwgt):
     return int(lib().or_gain_bucket_float(int(gx), int(vwgt)))
+
+
+if __name__ == "__main__":
+    print(build(force=True))
