@@ -425,7 +425,10 @@ def run_ours(args, world, rank, local):
     wl = WORKLOADS[args.workload]
     g = make_graph(H, wl, args.seed)
     edges = g.m // 2
-    ctx = H.Context(local, H.arena_estimate(g.n, g.m, g.ew is not None, g.vw is not None))
+    # mapping (HM) runs each hierarchy level's sub-solves concurrently in the
+    # arena's free space: give it twice the single-solve estimate
+    scale = 2 if wl["task"] == "map" else 1
+    ctx = H.Context(local, scale * H.arena_estimate(g.n, g.m, g.ew is not None, g.vw is not None))
     for t in args.tune:
         name, value = t.split("=")
         ctx.tune(name, int(value))

@@ -81,12 +81,27 @@ __device__ __forceinline__ PickLocal pick_local(const DGraph &g, const u32 *vcma
     const u64 beg = g.rowptr[u];
     const u32 len = g.rowlen[u];
     PickLocal p{false, 0, 0, SENTINEL};
-    for (u32 t = tid; t < len; t += nthreads) {
-        const u32 v = g.adj[beg + t];
-        if (!INITIAL && ld_vc<COH>(&vcmap[v]) != SENTINEL) continue;
-        const s32 w = g.ew ? g.ew[beg + t] : 0;
-        const u32 tb = xorshift32(v + r);
-        if (!p.found || w > p.w || (w == p.w && tb >= p.tb)) p = PickLocal{true, w, tb, v};
+    // four entries per thread are loaded and their match state gathered
+    // before they are compared (entries are visited in the same order)
+    for (u32 t0 = tid; t0 < len; t0 += 4 * nthreads) {
+        u32 vs[4];
+        s32 ws[4];
+        bool ok[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const u32 t = t0 + j * nthreads;
+            vs[j] = t < len ? g.adj[beg + t] : SENTINEL;
+            ws[j] = (t < len && g.ew) ? g.ew[beg + t] : 0;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            ok[j] = vs[j] != SENTINEL && (INITIAL || ld_vc<COH>(&vcmap[vs[j]]) == SENTINEL);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!ok[j]) continue;
+            const u32 tb = xorshift32(vs[j] + r);
+            if (!p.found || ws[j] > p.w || (ws[j] == p.w && tb >= p.tb)) p = PickLocal{true, ws[j], tb, vs[j]};
+        }
     }
     return p;
 }

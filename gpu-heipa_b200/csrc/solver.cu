@@ -187,7 +187,7 @@ struct HmTask {
 // and sorting buffers; the subgraph itself lives in the main arena).
 size_t worker_bytes(const DGraph &g) { return 96 * (size_t) g.m + 256 * (size_t) g.n + (64ull << 20); }
 
-constexpr size_t HM_MAX_WORKERS = 16;
+constexpr size_t HM_MAX_WORKERS = 32;
 
 // Runs fn(ctx_w, task) for every task. The sub-solves are independent and
 // deterministic, so they run concurrently on worker contexts (one host
