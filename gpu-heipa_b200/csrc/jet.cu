@@ -750,7 +750,7 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
 
 // When the moved rows hold at least inval_all_min entries, nearly every cache
 // is invalidated anyway: the delta kernels then skip the scattered resets and
-// k_inval_all resets all caches with one sequential fill. Only enabled where a
+// k_inval_unmark resets all caches with one sequential fill. Only enabled where a
 // recomputed gain equals the cached one for every vertex whose neighbourhood
 // did not change (a fixed filter ratio per level, or the mapping objective).
 __device__ __forceinline__ bool scattered_inval(const JArgs &a) {
