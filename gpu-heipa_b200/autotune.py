@@ -21,9 +21,11 @@ CANDIDATES = {
     "order_small_n": [0, 4096, 16384, 65536],
     "match_coop_max_n": [0, 1 << 15, 1 << 17, 1 << 19],
     "match_coop_max_m": [0, 1 << 19, 1 << 21, 1 << 23],
+    "jet_fused_max_n": [0, 2048, 8192, 32768, 65536],
+    "jet_fused_max_m": [1 << 16, 1 << 18, 1 << 20],
 }
 DEFAULTS = {"jet_graph_max_m": 1 << 24, "order_small_n": 16384, "match_coop_max_n": 1 << 17,
-            "match_coop_max_m": 1 << 21}
+            "match_coop_max_m": 1 << 21, "jet_fused_max_n": 8192, "jet_fused_max_m": 1 << 18}
 
 
 def _time(ctx, graphs, ks, config, seed, repeats):

@@ -130,6 +130,8 @@ struct Tunables {
     u32 order_small_n = 16384;         // single-block rebalance ordering up to this many vertices
     u32 match_coop_max_n = 1u << 17;   // cooperative matching loop up to this many vertices ...
     u64 match_coop_max_m = 1ull << 21; // ... and entries
+    u32 jet_fused_max_n = 8192;        // whole Jet level loop in one block up to this many vertices ...
+    u64 jet_fused_max_m = 1ull << 18;  // ... and entries
 };
 
 struct Ctx {

@@ -117,6 +117,14 @@ struct Grp {
     }
 };
 
+// Loads of Jet state (labels, targets, gains) that the calling kernel does not
+// write go through the non-coherent path (NC); the fused small-level kernel,
+// which writes them between its phases, uses plain loads.
+template<bool NC, typename T>
+__device__ __forceinline__ T ldj(const T *p) {
+    return NC ? __ldg(p) : *p;
+}
+
 __device__ __forceinline__ u32 thash(u32 key, u32 mask) { return (key * 2654435761u >> 7) & mask; }
 
 __device__ __forceinline__ u32 table_mask_for(u32 len, u32 k, u32 cap) {
@@ -128,7 +136,7 @@ __device__ __forceinline__ u32 table_mask_for(u32 len, u32 k, u32 cap) {
 
 // Aggregates conn(u, .) into the group's hashed table (cleared on entry).
 // Four entries per thread are loaded before they are inserted.
-template<bool BLK>
+template<bool BLK, bool NC = true>
 __device__ __forceinline__ void table_build(const JArgs &a, u32 u, u32 *tk, s32 *tv, u32 mask) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     const u32 len = __ldg(&a.g.rowlen[u]);
@@ -144,7 +152,7 @@ __device__ __forceinline__ void table_build(const JArgs &a, u32 u, u32 *tk, s32 
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-            if (bb[j] != EMPTY) bb[j] = __ldg(&a.map[bb[j]]);
+            if (bb[j] != EMPTY) bb[j] = ldj<NC>(&a.map[bb[j]]);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const u32 b = bb[j];
@@ -180,7 +188,7 @@ __device__ __forceinline__ void table_clear(u32 *tk, s32 *tv, u32 mask) {
 // connection; weights are positive), so an entry costs one shared-memory add
 // and no compare-and-swap. Four entries per thread are loaded (ids, then
 // labels) before any table update, which keeps four gathers in flight.
-template<bool BLK>
+template<bool BLK, bool NC = true>
 __device__ __forceinline__ void dtable_build_range(const JArgs &a, u32 u, s32 *tv, u32 from, u32 len) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     const u32 gs = Grp<BLK>::size(), tid = Grp<BLK>::tid();
@@ -195,7 +203,7 @@ __device__ __forceinline__ void dtable_build_range(const JArgs &a, u32 u, s32 *t
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-            if (b[j] != EMPTY) b[j] = __ldg(&a.map[b[j]]);
+            if (b[j] != EMPTY) b[j] = ldj<NC>(&a.map[b[j]]);
 #pragma unroll
         for (int j = 0; j < 4; ++j)
             if (b[j] != EMPTY) atomicAdd(&tv[b[j]], w[j]);
@@ -203,9 +211,9 @@ __device__ __forceinline__ void dtable_build_range(const JArgs &a, u32 u, s32 *t
     Grp<BLK>::sync();
 }
 
-template<bool BLK>
+template<bool BLK, bool NC = true>
 __device__ __forceinline__ void dtable_build(const JArgs &a, u32 u, s32 *tv) {
-    dtable_build_range<BLK>(a, u, tv, 0, __ldg(&a.g.rowlen[u]));
+    dtable_build_range<BLK, NC>(a, u, tv, 0, __ldg(&a.g.rowlen[u]));
 }
 
 template<bool BLK>
@@ -216,15 +224,15 @@ __device__ __forceinline__ void dtable_clear(s32 *tv, u32 k) {
 }
 
 // Connectivity table of one row: direct-indexed (DIRECT) or hashed.
-template<bool BLK, bool DIRECT>
+template<bool BLK, bool DIRECT, bool NC = true>
 struct ConnTable {
     u32 *tk;
     s32 *tv;
     u32 mask;  // hashed: slots - 1
     u32 k;
     __device__ __forceinline__ void build(const JArgs &a, u32 u) {
-        if (DIRECT) dtable_build<BLK>(a, u, tv);
-        else table_build<BLK>(a, u, tk, tv, mask);
+        if (DIRECT) dtable_build<BLK, NC>(a, u, tv);
+        else table_build<BLK, NC>(a, u, tk, tv, mask);
     }
     __device__ __forceinline__ u32 slots() const { return DIRECT ? k : mask + 1; }
     __device__ __forceinline__ u32 key(u32 s) const { return DIRECT ? (tv[s] != 0 ? s : EMPTY) : tk[s]; }
@@ -246,6 +254,7 @@ struct TRow {
 // loads in flight instead of a chain of JT), then equal blocks are merged into
 // their first occurrence. Labels are not written by the kernels that call
 // this, so they are read through the non-coherent path.
+template<bool NC = true>
 __device__ __forceinline__ void trow_build(const JArgs &a, u32 u, TRow &r) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     const u32 len = __ldg(&a.g.rowlen[u]);
@@ -256,7 +265,7 @@ __device__ __forceinline__ void trow_build(const JArgs &a, u32 u, TRow &r) {
     }
 #pragma unroll
     for (int s = 0; s < (int) JT; ++s)
-        if (r.b[s] != EMPTY) r.b[s] = __ldg(&a.map[r.b[s]]);
+        if (r.b[s] != EMPTY) r.b[s] = ldj<NC>(&a.map[r.b[s]]);
 #pragma unroll
     for (int s = 1; s < (int) JT; ++s) {
 #pragma unroll
@@ -310,9 +319,10 @@ __device__ __forceinline__ void lp_finish_map(const JArgs &a, u32 u, unsigned lo
     lp_store(a, u, best, gain);
 }
 
+template<bool NC = true>
 __device__ __forceinline__ void lp_thread(const JArgs &a, u32 u, u32 ratio) {
     TRow r;
-    trow_build(a, u, r);
+    trow_build<NC>(a, u, r);
     const u32 o = a.map[u];
     unsigned long long bk = 0;
     if (!a.code) {
@@ -343,8 +353,8 @@ __device__ __forceinline__ void lp_thread(const JArgs &a, u32 u, u32 ratio) {
 }
 
 // Best block of u from its built connectivity table T (clears T).
-template<bool BLK, bool DIRECT>
-__device__ __forceinline__ void lp_finish_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT> T,
+template<bool BLK, bool DIRECT, bool NC = true>
+__device__ __forceinline__ void lp_finish_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT, NC> T,
                                                 unsigned long long *smu, long long *sms) {
     const u32 o = a.map[u];
     unsigned long long bk = 0;
@@ -379,11 +389,11 @@ __device__ __forceinline__ void lp_finish_group(const JArgs &a, u32 u, u32 ratio
     T.clear();
 }
 
-template<bool BLK, bool DIRECT>
-__device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT> T,
+template<bool BLK, bool DIRECT, bool NC = true>
+__device__ __forceinline__ void lp_group(const JArgs &a, u32 u, u32 ratio, ConnTable<BLK, DIRECT, NC> T,
                                          unsigned long long *smu, long long *sms) {
     T.build(a, u);
-    lp_finish_group<BLK, DIRECT>(a, u, ratio, T, smu, sms);
+    lp_finish_group<BLK, DIRECT, NC>(a, u, ratio, T, smu, sms);
 }
 
 // Direct-indexed tables are used when k fits the table and, for the mapping
@@ -591,6 +601,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_filter(JArgs a) {
 // over a group of threads (wrap-around s32 arithmetic). The gains, targets
 // and labels read here are not written by the afterburner kernels, so they
 // are gathered through the non-coherent path, four entries at a time.
+template<bool NC = true>
 __device__ __forceinline__ s32 ab_range(const JArgs &a, u32 u, s32 ug, u32 ou, u32 nu, u32 from, u32 to, u32 tid,
                                         u32 nthreads) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
@@ -609,13 +620,13 @@ __device__ __forceinline__ s32 ab_range(const JArgs &a, u32 u, s32 ug, u32 ou, u
         // the gains, still four at a time
         bool first[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) vg[j] = v[j] != SENTINEL ? __ldg(&a.gain1[v[j]]) : 0;
+        for (int j = 0; j < 4; ++j) vg[j] = v[j] != SENTINEL ? ldj<NC>(&a.gain1[v[j]]) : 0;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
             if (first[j]) {
-                nv[j] = __ldg(&a.dest_part[v[j]]);
-                ov[j] = __ldg(&a.map[v[j]]);
+                nv[j] = ldj<NC>(&a.dest_part[v[j]]);
+                ov[j] = ldj<NC>(&a.map[v[j]]);
             }
         }
 #pragma unroll
@@ -707,13 +718,14 @@ __global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
 // are read through the non-coherent path; four entries per thread are loaded
 // (ids, then labels, then old labels of moved neighbours) before the cache
 // resets are stored, which keeps four dependent gathers in flight.
+template<bool NC = true>
 __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 nthreads,
                                                  bool inval) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
-    const u32 x = __ldg(&a.map[u]);
+    const u32 x = ldj<NC>(&a.map[u]);
     const bool um = (x & MOVED) != 0;
     const u32 nu = x & ~MOVED;
-    const u32 ou = um ? __ldg(&a.dest_part[u]) : nu;
+    const u32 ou = um ? ldj<NC>(&a.dest_part[u]) : nu;
     long long acc = 0;
     for (u32 t0 = from + tid; t0 < to; t0 += 4 * nthreads) {
         u32 v[4], xv[4], ov[4];
@@ -726,9 +738,9 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
         }
         if (um) {
 #pragma unroll
-            for (int j = 0; j < 4; ++j) xv[j] = v[j] != SENTINEL ? __ldg(&a.map[v[j]]) : 0;
+            for (int j = 0; j < 4; ++j) xv[j] = v[j] != SENTINEL ? ldj<NC>(&a.map[v[j]]) : 0;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) ov[j] = (xv[j] & MOVED) ? __ldg(&a.dest_part[v[j]]) : (xv[j] & ~MOVED);
+            for (int j = 0; j < 4; ++j) ov[j] = (xv[j] & MOVED) ? ldj<NC>(&a.dest_part[v[j]]) : (xv[j] & ~MOVED);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (v[j] == SENTINEL) continue;
@@ -945,10 +957,10 @@ __device__ __forceinline__ bool rb_qualifies(const JArgs &a, const RbArgs &r, u3
     return (s64) vw <= 2 * (s64) maxv && (s64) vw < 2 * (ow - r.opt);
 }
 
-template<bool STRONG>
+template<bool STRONG, bool NC = true>
 __device__ __forceinline__ void rb_thread(const JArgs &a, const RbArgs &r, u32 u, u32 o) {
     TRow row;
-    trow_build(a, u, row);
+    trow_build<NC>(a, u, row);
     s32 own = 0, sum = 0, count = 0;
     unsigned long long bk = 0;
 #pragma unroll
@@ -973,9 +985,10 @@ __device__ __forceinline__ void rb_thread(const JArgs &a, const RbArgs &r, u32 u
     else weak_finish(a, r, u, o, own, bk);
 }
 
-template<bool STRONG, bool BLK, bool DIRECT>
-__device__ __forceinline__ void rb_finish_group(const JArgs &a, const RbArgs &r, u32 u, ConnTable<BLK, DIRECT> T,
-                                                unsigned long long *smu, long long *sms) {
+template<bool STRONG, bool BLK, bool DIRECT, bool NC = true>
+__device__ __forceinline__ void rb_finish_group(const JArgs &a, const RbArgs &r, u32 u,
+                                                ConnTable<BLK, DIRECT, NC> T, unsigned long long *smu,
+                                                long long *sms) {
     const u32 o = a.map[u];
     long long own = 0, sum = 0, count = 0;
     unsigned long long bk = 0;
@@ -1012,11 +1025,11 @@ __device__ __forceinline__ void rb_finish_group(const JArgs &a, const RbArgs &r,
     T.clear();
 }
 
-template<bool STRONG, bool BLK, bool DIRECT>
-__device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u, ConnTable<BLK, DIRECT> T,
+template<bool STRONG, bool BLK, bool DIRECT, bool NC = true>
+__device__ __forceinline__ void rb_group(const JArgs &a, const RbArgs &r, u32 u, ConnTable<BLK, DIRECT, NC> T,
                                          unsigned long long *smu, long long *sms) {
     T.build(a, u);
-    rb_finish_group<STRONG, BLK, DIRECT>(a, r, u, T, smu, sms);
+    rb_finish_group<STRONG, BLK, DIRECT, NC>(a, r, u, T, smu, sms);
 }
 
 template<bool STRONG>
@@ -1132,7 +1145,7 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub(JArgs a, u32 ratio, RbArgs r) 
 }
 
 // underloaded_blocks (:614-627): ordered list of blocks below max_b_w.
-__global__ void k_under(const s32 *bw, u32 k, s32 max_b_w, u32 *under, u32 *n_under) {
+__device__ __forceinline__ void under_block(const s32 *bw, u32 k, s32 max_b_w, u32 *under, u32 *n_under) {
     __shared__ u32 sm[32];
     u32 carry = 0;
     for (u32 base = 0; base < k; base += blockDim.x) {
@@ -1146,8 +1159,12 @@ __global__ void k_under(const s32 *bw, u32 k, s32 max_b_w, u32 *under, u32 *n_un
     if (threadIdx.x == 0) *n_under = carry;
 }
 
+__global__ void k_under(const s32 *bw, u32 k, s32 max_b_w, u32 *under, u32 *n_under) {
+    under_block(bw, k, max_b_w, under, n_under);
+}
+
 // find max size (:377-385): largest free capacity below max_b_w (INT32_MIN if none)
-__global__ void k_maxv(const s32 *bw, u32 k, s32 max_b_w, int *out) {
+__device__ __forceinline__ void maxv_block(const s32 *bw, u32 k, s32 max_b_w, int *out) {
     s32 m = INT32_MIN;
     for (u32 b = threadIdx.x; b < k; b += blockDim.x)
         if (bw[b] < max_b_w && max_b_w - bw[b] > m) m = max_b_w - bw[b];
@@ -1161,6 +1178,8 @@ __global__ void k_maxv(const s32 *bw, u32 k, s32 max_b_w, int *out) {
         *out = r;
     }
 }
+
+__global__ void k_maxv(const s32 *bw, u32 k, s32 max_b_w, int *out) { maxv_block(bw, k, max_b_w, out); }
 
 // B(x) for x = p * width, p in [0, k]: weight of candidates with key < x.
 __global__ void k_bounds(const u32 *skeys, const long long *prefix, const u32 *d_c, u32 k, u32 width, long long *B) {
@@ -1413,14 +1432,21 @@ __device__ bool block_sort_pairs(u32 *k0, u32 *v0, u32 *k1, u32 *v1, u32 cnt, in
     return flipped;
 }
 
+// Whole-block body (OB threads); leaves the move count in cnt[ST_MOVES].
+struct OrderSmem {
+    u32 offs[256];
+    u32 wc[OB / 32][256];
+    u32 scan_sm[32];
+    long long lsm[32];
+    u32 cnt_sm[3];  // candidates, moves, fallbacks
+};
+
 template<bool STRONG>
-__global__ void __launch_bounds__(OB, 1) k_order_small(JArgs a, RbArgs r, u32 width, int key_bits, OrderScratch S,
-                                                        s32 max_b_w) {
-    __shared__ u32 offs[256];
-    __shared__ u32 wc[OB / 32][256];
-    __shared__ u32 scan_sm[32];
-    __shared__ long long lsm[32];
-    __shared__ u32 cnt_sm[3];  // candidates, moves, fallbacks
+__device__ void order_small_body(const JArgs &a, const RbArgs &r, u32 width, int key_bits, const OrderScratch &S,
+                                 s32 max_b_w, OrderSmem &sm) {
+    u32 *offs = sm.offs, *scan_sm = sm.scan_sm, *cnt_sm = sm.cnt_sm;
+    u32 (*wc)[256] = sm.wc;
+    long long *lsm = sm.lsm;
     const u32 tid = threadIdx.x, n = a.g.n;
     if (tid < 3) cnt_sm[tid] = 0;
     if (STRONG)
@@ -1518,6 +1544,306 @@ __global__ void __launch_bounds__(OB, 1) k_order_small(JArgs a, RbArgs r, u32 wi
     if (tid == 0) a.st->cnt[ST_MOVES] = nm;
 }
 
+template<bool STRONG>
+__global__ void __launch_bounds__(OB, 1) k_order_small(JArgs a, RbArgs r, u32 width, int key_bits, OrderScratch S,
+                                                        s32 max_b_w) {
+    __shared__ OrderSmem sm;
+    order_small_body<STRONG>(a, r, width, key_bits, S, max_b_w, sm);
+}
+
+// ---- fused refinement of small levels -------------------------------------------------
+
+// Levels of at most Tunables::jet_fused_max_n vertices run the whole level loop
+// of jet_refine in one 1024-thread block: the iteration control (ratios,
+// weak/strong switching, best-labelling tracking), and per iteration the same
+// steps as the per-kernel path (gain pass, filter, afterburner, weak or
+// strong rebalancing with the one-block ordering, perform). Everything stays
+// on one SM: counters and block weights live in shared memory, Jet state is
+// read with plain loads after __syncthreads(), so writes of earlier phases are
+// visible. The result equals the per-kernel path's (a parity test forces both).
+constexpr int FB = OB;                  // threads of the fused kernel (= the ordering block)
+constexpr u32 FUSED_MAX_N = 1u << 16;   // upper bound of Tunables::jet_fused_max_n
+constexpr u32 FUSED_AB_THREAD = 32;     // afterburner / delta rows handled by one thread
+
+struct FusedCtl {
+    u32 n_ratios;
+    u32 ratios[17];
+    s32 lmax;
+    u32 promap;
+    long long obj;  // in: objective of the input labelling; out: best objective
+    s32 maxw;       // in / out: maximum block weight
+    u32 iterations; // out: Jet iterations run
+};
+
+struct FusedArgs {
+    RbArgs weak, strong;
+    u32 width;
+    int bits_weak, bits_strong;
+    OrderScratch S;
+    u32 *under; // writable alias of weak.under
+    u32 *part;  // receives the best labelling
+};
+
+// Block weights kept in shared memory during the fused kernel and mirrored to
+// a.bw (plain stores) for the functions that read it.
+__device__ __forceinline__ void fused_publish_bw(const JArgs &a, const s32 *sbw) {
+    for (u32 b = threadIdx.x; b < a.k; b += blockDim.x) a.bw[b] = sbw[b];
+    __syncthreads();
+}
+
+__device__ __forceinline__ long long block_sum_ll(long long v, long long *sm) {
+    v = warp_sum<long long>(v);
+    if (lane_id() == 0) sm[warp_in_block()] = v;
+    __syncthreads();
+    long long r = 0;
+    if (threadIdx.x == 0) {
+        for (u32 w = 0; w < (blockDim.x >> 5); ++w) r += sm[w];
+        sm[32] = r;
+    }
+    __syncthreads();
+    r = sm[32];
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(FB, 1) k_jet_fused(JArgs a, FusedArgs F, FusedCtl *ctl) {
+    extern __shared__ s32 fsm[];
+    s32 *wtab = fsm + (u32) warp_in_block() * a.k;  // per-warp direct table
+    s32 *btab = fsm + 32u * a.k;                    // block table
+    s32 *sbw = fsm + 33u * a.k;                     // block weights
+    __shared__ u32 sc[8];
+    __shared__ long long sl[33];
+    __shared__ unsigned long long smu[33];
+    __shared__ long long sms[33];
+    __shared__ int si[2];
+    __shared__ OrderSmem osm;
+    const u32 tid = threadIdx.x, lane = lane_id(), warp = warp_in_block(), n = a.g.n, k = a.k;
+    for (u32 i = tid; i < 33u * k; i += FB) fsm[i] = 0;
+    for (u32 b = tid; b < k; b += FB) sbw[b] = a.bw[b];
+    __syncthreads();
+    const ConnTable<false, true, false> WT{nullptr, wtab, 0, k};
+    const ConnTable<true, true, false> BT{nullptr, btab, 0, k};
+    const bool promap = ctl->promap != 0;
+    const s32 lmax = ctl->lmax;
+    long long obj = ctl->obj, best_obj = obj;
+    s32 maxw = ctl->maxw, best_max = maxw;
+    u32 iterations = 0;
+    for (u32 ri = 0; ri < ctl->n_ratios; ++ri) {
+        const u32 ratio = ctl->ratios[ri];
+        u32 balance_iteration = 0, iteration = 0;
+        while (iteration < JET_MAX_ITERATIONS) {
+            iteration += 1;
+            ++iterations;
+            bool lp_iter = false;
+            int step;
+            if (!promap) {
+                if (maxw <= lmax) {
+                    step = 0;
+                    lp_iter = true;
+                    balance_iteration = 0;
+                } else {
+                    step = balance_iteration < JET_MAX_WEAK_ITERATIONS ? 1 : 2;
+                }
+            } else {
+                if (maxw <= lmax) {
+                    step = 0;
+                    lp_iter = true;
+                    balance_iteration = 0;
+                } else {
+                    balance_iteration++;
+                    step = balance_iteration < JET_MAX_WEAK_ITERATIONS ? 1 : 2;
+                }
+            }
+            if (tid < 8) sc[tid] = 0;
+            __syncthreads();
+            if (step == 0) {
+                // gain pass (jet_lp :193-238): cached targets, else recompute
+                for (u32 u = tid; u < n; u += FB) {
+                    const u32 dc = a.dest_cache[u];
+                    if (dc != NULL_PART) {
+                        a.dest_part[u] = dc;
+                        continue;
+                    }
+                    const int cls = table_tier(a.g.rowlen[u], k);
+                    if (cls == 0) lp_thread<false>(a, u, ratio);
+                    else if (cls == 1) a.heavy[atomicAdd(&sc[0], 1u)] = u;
+                    else a.heavy2[atomicAdd(&sc[1], 1u)] = u;
+                }
+                __syncthreads();
+                for (u32 i = warp; i < sc[0]; i += FB / 32) lp_group<false, true, false>(a, a.heavy[i], ratio, WT, nullptr, nullptr);
+                __syncthreads();
+                for (u32 i = 0; i < sc[1]; ++i) lp_group<true, true, false>(a, a.heavy2[i], ratio, BT, smu, sms);
+                __syncthreads();
+                // filter (:247-258)
+                for (u32 u = tid; u < n; u += FB) {
+                    if (a.dest_part[u] != NO_MOVE && a.lock[u] == 0) {
+                        a.gain1[u] = a.gain_cache[u];
+                        a.cand[atomicAdd(&sc[2], 1u)] = u;
+                    } else {
+                        a.gain1[u] = GAIN_MIN;
+                        a.lock[u] = 0;
+                    }
+                }
+                __syncthreads();
+                // afterburner: short rows by a thread, longer ones by a warp
+                const u32 nc = sc[2];
+                for (u32 i = tid; i < nc; i += FB) {
+                    const u32 u = a.cand[i];
+                    const u32 len = a.g.rowlen[u];
+                    if (len <= FUSED_AB_THREAD) {
+                        const s32 ug = a.gain1[u];
+                        if (wadd(ug, ab_range<false>(a, u, ug, a.map[u], a.dest_part[u], 0, len, 0, 1)) >= 0) {
+                            a.lock[u] = 1;
+                            a.moves[atomicAdd(&sc[3], 1u)] = u;
+                        }
+                    } else {
+                        a.heavy[atomicAdd(&sc[4], 1u)] = u;
+                    }
+                }
+                __syncthreads();
+                for (u32 i = warp; i < sc[4]; i += FB / 32) {
+                    const u32 u = a.heavy[i];
+                    const s32 ug = a.gain1[u];
+                    const s32 change = (s32) warp_sum<u32>(
+                        (u32) ab_range<false>(a, u, ug, a.map[u], a.dest_part[u], 0, a.g.rowlen[u], lane, 32));
+                    if (lane == 0 && wadd(ug, change) >= 0) {
+                        a.lock[u] = 1;
+                        a.moves[atomicAdd(&sc[3], 1u)] = u;
+                    }
+                }
+                __syncthreads();
+                if (tid == 0) a.st->cnt[ST_MOVES] = sc[3];
+                __syncthreads();
+            } else {
+                // rebalancing picks (rebalance_weak :592-751 / rebalance_strong :356-590)
+                const bool strong = step == 2;
+                const RbArgs &r = strong ? F.strong : F.weak;
+                if (strong) maxv_block(a.bw, k, r.max_b_w, &a.st->imax[1]);
+                else under_block(a.bw, k, r.max_b_w, F.under, &a.st->cnt[ST_AUX]);
+                __syncthreads();
+                const s32 maxv = a.st->imax[1];
+                for (u32 u = tid; u < n; u += FB) {
+                    const u32 o = a.map[u];
+                    const bool q = strong ? rb_qualifies<true>(a, r, o, g_vw(a.g, u), maxv)
+                                          : rb_qualifies<false>(a, r, o, g_vw(a.g, u), maxv);
+                    if (!q) {
+                        if (!strong) a.dest_part[u] = o;
+                        r.keys[u] = NOKEY;
+                        continue;
+                    }
+                    const int cls = table_tier(a.g.rowlen[u], k);
+                    if (cls == 0) {
+                        if (strong) rb_thread<true, false>(a, r, u, o);
+                        else rb_thread<false, false>(a, r, u, o);
+                    } else if (cls == 1) {
+                        a.heavy[atomicAdd(&sc[0], 1u)] = u;
+                    } else {
+                        a.heavy2[atomicAdd(&sc[1], 1u)] = u;
+                    }
+                }
+                __syncthreads();
+                for (u32 i = warp; i < sc[0]; i += FB / 32) {
+                    if (strong) rb_group<true, false, true, false>(a, r, a.heavy[i], WT, nullptr, nullptr);
+                    else rb_group<false, false, true, false>(a, r, a.heavy[i], WT, nullptr, nullptr);
+                }
+                __syncthreads();
+                for (u32 i = 0; i < sc[1]; ++i) {
+                    if (strong) rb_group<true, true, true, false>(a, r, a.heavy2[i], BT, smu, sms);
+                    else rb_group<false, true, true, false>(a, r, a.heavy2[i], BT, smu, sms);
+                }
+                __syncthreads();
+                if (strong) order_small_body<true>(a, r, F.width, F.bits_strong, F.S, r.max_b_w, osm);
+                else order_small_body<false>(a, r, F.width, F.bits_weak, F.S, r.max_b_w, osm);
+                __syncthreads();
+            }
+            const u32 nm = a.st->cnt[ST_MOVES];
+            // perform_moves (:753-924): labels with the moved bit, block weights
+            long long entries = 0;
+            for (u32 i = tid; i < nm; i += FB) {
+                const u32 u = a.moves[i];
+                const u32 ou = a.map[u], nu = a.dest_part[u];
+                const s32 w = g_vw(a.g, u);
+                if (ou != nu) {
+                    atomicSub(&sbw[ou], w);
+                    atomicAdd(&sbw[nu], w);
+                }
+                a.map[u] = ou != nu ? (nu | MOVED) : nu;
+                a.dest_part[u] = ou;
+                a.dest_cache[u] = NULL_PART;
+                entries += a.g.rowlen[u];
+            }
+            entries = block_sum_ll(entries, sl);
+            s32 m = 0;
+            for (u32 b = tid; b < k; b += FB) m = sbw[b] > m ? sbw[b] : m;
+            m = __reduce_max_sync(FULL, m);
+            if (lane == 0) sl[warp] = m;
+            __syncthreads();
+            if (tid == 0) {
+                s32 r = 0;
+                for (u32 w = 0; w < FB / 32; ++w) r = (s32) sl[w] > r ? (s32) sl[w] : r;
+                si[0] = r;
+            }
+            __syncthreads();
+            const s32 new_maxw = si[0];
+            const bool inval = (unsigned long long) entries < a.inval_all_min;
+            // exact objective change and the neighbours' cache resets
+            long long acc = 0;
+            for (u32 i = tid; i < nm; i += FB) {
+                const u32 u = a.moves[i];
+                const u32 len = a.g.rowlen[u];
+                if (len <= FUSED_AB_THREAD) acc += delta_range<false>(a, u, 0, len, 0, 1, inval);
+                else a.heavy[atomicAdd(&sc[5], 1u)] = u;
+            }
+            __syncthreads();
+            for (u32 i = warp; i < sc[5]; i += FB / 32) {
+                const u32 u = a.heavy[i];
+                acc += delta_range<false>(a, u, 0, a.g.rowlen[u], lane, 32, inval);
+            }
+            const long long d = block_sum_ll(acc, sl);
+            if (!inval)
+                for (u32 u = tid; u < n; u += FB) a.dest_cache[u] = NULL_PART;
+            for (u32 i = tid; i < nm; i += FB) a.map[a.moves[i]] &= ~MOVED;
+            fused_publish_bw(a, sbw);  // includes __syncthreads()
+            // control (jet_label_propagation.h:966-1030, promap :1250-1305)
+            if (!promap) {
+                if (nm == 0) {
+                    if (lp_iter) break;
+                    if (balance_iteration < JET_MAX_WEAK_ITERATIONS) {
+                        balance_iteration = JET_MAX_WEAK_ITERATIONS;
+                        continue;
+                    }
+                    break;
+                }
+                if (!lp_iter) balance_iteration++;
+            } else if (nm == 0) {
+                continue;
+            }
+            obj += promap ? d : d / 2;
+            maxw = new_maxw;
+            const bool leq = promap ? (maxw < best_max) : (maxw <= best_max);
+            bool copy = false;
+            if (best_max > lmax && maxw < best_max) {
+                copy = true;
+                iteration = 0;
+            } else if (obj < best_obj && (maxw <= lmax || leq)) {
+                if (1000 * obj < 999 * best_obj) iteration = 0;  // PHI = 0.999
+                copy = true;
+            }
+            if (copy) {
+                for (u32 u = tid; u < n; u += FB) F.part[u] = a.map[u];
+                best_obj = obj;
+                best_max = maxw;
+                __syncthreads();
+            }
+        }
+    }
+    if (tid == 0) {
+        ctl->obj = best_obj;
+        ctl->maxw = best_max;
+        ctl->iterations = iterations;
+    }
+}
+
 // ---- objectives ------------------------------------------------------------------
 
 __global__ void k_objective(DGraph g, const u32 *part, const u32 *code, const s32 *bitdist, unsigned long long *out) {
@@ -1600,6 +1926,8 @@ void set_big_smem() {
     HP_CUDA(cudaFuncSetAttribute(k_lp_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     HP_CUDA(cudaFuncSetAttribute(k_rb_block<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     HP_CUDA(cudaFuncSetAttribute(k_rb_block<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    HP_CUDA(cudaFuncSetAttribute(k_jet_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) (34 * JW_SLOTS * sizeof(s32))));
     done.push_back(dev);
 }
 
@@ -2072,6 +2400,60 @@ void JetLevel::run_step(int kind, u32 ratio_pct) {
     c.sync();
 }
 
+// The whole level loop in one k_jet_fused launch (warp_direct levels of at
+// most FUSED_MAX_N vertices); writes the best labelling to part.
+static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &ratios, bool promap, u32 *part,
+                             s64 &obj, s32 &maxw) {
+    const u32 n = L.g.n, k = L.k;
+    const s32 opt = (L.g_weight + (s32) (k - 1)) / (s32) k;
+    u32 sections, width;
+    sections_of(n, k, sections, width);
+    FusedArgs F{};
+    F.weak.opt = F.strong.opt = opt;
+    F.weak.max_b_w = std::max<s32>(L.lmax - 100, (s32) ((99 * (s64) L.lmax) / 100));
+    F.strong.max_b_w = std::max<s32>(opt + 1, (s32) ((99 * (s64) L.lmax) / 100));
+    F.weak.sections = F.strong.sections = sections;
+    F.under = ctx.balloc<u32>(k);
+    F.weak.under = F.under;
+    F.weak.keys = F.strong.keys = ctx.balloc<u32>(n);
+    F.width = width;
+    F.bits_weak = bits_for((u64) MAX_BUCKETS * k * sections + 1);
+    F.bits_strong = bits_for((u64) MAX_BUCKETS * k * sections + 2);
+    OrderScratch &S = F.S;
+    S.cands = ctx.balloc<u32>(n);
+    S.ck = ctx.balloc<u32>(n);
+    S.cands2 = ctx.balloc<u32>(n);
+    S.ck2 = ctx.balloc<u32>(n);
+    S.prefix = ctx.balloc<long long>((u64) n + 1);
+    S.B = ctx.balloc<long long>((u64) k + 1);
+    S.ea = ctx.balloc<long long>(k);
+    S.es = ctx.balloc<long long>((u64) k + 1);
+    S.mpre = ctx.balloc<long long>((u64) n + 1);
+    S.fail = ctx.balloc<u32>(n);
+    S.fail2 = ctx.balloc<u32>(n);
+    F.part = part;
+    FusedCtl h{};
+    h.n_ratios = (u32) ratios.size();
+    for (size_t i = 0; i < ratios.size() && i < 17; ++i) h.ratios[i] = ratios[i];
+    h.lmax = L.lmax;
+    h.promap = promap ? 1u : 0u;
+    h.obj = obj;
+    h.maxw = maxw;
+    FusedCtl *d = ctx.balloc<FusedCtl>(1);
+    HP_CUDA(cudaMemcpyAsync(d, &h, sizeof(FusedCtl), cudaMemcpyHostToDevice, ctx.stream));
+    ctx.zero_counters();
+    {
+        KernTimer kt(ctx, "k_jet_fused");
+        k_jet_fused<<<1, FB, 34 * k * sizeof(s32), ctx.stream>>>(make_args(L), F, d); note_launch();
+    }
+    HP_LAUNCH_CHECK();
+    HP_CUDA(cudaMemcpyAsync(&h, d, sizeof(FusedCtl), cudaMemcpyDeviceToHost, ctx.stream));
+    const DevStatus &st = ctx.read_status();
+    if (st.err) throw HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
+    obj = h.obj;
+    maxw = h.maxw;
+}
+
 void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultra, u32 level, s64 &obj, s32 &maxw,
                 const DistOracle *D) {
     if (g.n == 0 || k <= 1) return;
@@ -2088,6 +2470,11 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
     std::vector<u32> ratios;
     if (ultra && !promap) ratios = {85, 80, 75, 70, 65, 60, 55, 50, 45, 40, 35, 30, 25, 20, 15, 10, 5};
     else ratios = {level == 0 ? 25u : 75u};
+    if (L.warp_direct && g.n <= std::min<u32>(ctx.tune.jet_fused_max_n, FUSED_MAX_N) &&
+        g.m <= ctx.tune.jet_fused_max_m && !ctx.prof.enabled) {
+        jet_refine_fused(ctx, L, ratios, promap, part, obj, maxw);
+        return;
+    }
     for (u32 ratio: ratios) {
         u32 balance_iteration = 0, iteration = 0;
         while (iteration < JET_MAX_ITERATIONS) {

@@ -180,7 +180,10 @@ int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t
  * 0 = never), "order_small_n" (single-block rebalance ordering up to this many
  * vertices, at most 65536; 0 = never), "match_coop_max_n" / "match_coop_max_m"
  * (one cooperative launch for the matching loop of levels up to these sizes;
- * 0 = never). Unknown names return HP_ERR_ARG. No counterpart in the reference. */
+ * 0 = never), "jet_fused_max_n" / "jet_fused_max_m" (the whole refinement loop
+ * of a level in one single-block launch up to these sizes, vertices capped at
+ * 65536, when k <= 1024, or k <= 256 for the mapping objective; 0 = never).
+ * Unknown names return HP_ERR_ARG. No counterpart in the reference. */
 int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
 
 /* Enables CUDA-event timing of the contraction and Jet-gain kernels on ctx;

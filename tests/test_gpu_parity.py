@@ -280,7 +280,7 @@ def test_direct_launch_paths_equal(ctx):
     want_m, want_j = ctx.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, "HM", 3)
     c2 = H.Context(0, 2 << 30)
     try:
-        for name in ("jet_graph_max_m", "order_small_n", "match_coop_max_n", "match_coop_max_m"):
+        for name in ("jet_graph_max_m", "order_small_n", "match_coop_max_n", "match_coop_max_m", "jet_fused_max_n"):
             c2.tune(name, 0)
         part, cut = c2.partition(g, 64, 0.03, "default", 7)
         assert cut == want_c

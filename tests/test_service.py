@@ -78,7 +78,7 @@ def test_autotune_keeps_results(ctx):
     ks = [8, 16]
     before = [ctx.partition(g, k, 0.03, "default", 1) for g, k in zip(graphs, ks)]
     small = {"jet_graph_max_m": [0, 1 << 24], "order_small_n": [0, 4096], "match_coop_max_n": [0, 1 << 17],
-             "match_coop_max_m": [1 << 21]}
+             "match_coop_max_m": [1 << 21], "jet_fused_max_n": [0, 8192]}
     best = autotune.tune(ctx, graphs, ks, candidates=small, repeats=1)
     assert set(best) == set(autotune.DEFAULTS)
     after = [ctx.partition(g, k, 0.03, "default", 1) for g, k in zip(graphs, ks)]
