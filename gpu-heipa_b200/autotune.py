@@ -23,9 +23,11 @@ CANDIDATES = {
     "match_coop_max_m": [0, 1 << 19, 1 << 21, 1 << 23],
     "jet_fused_max_n": [0, 2048, 8192, 32768, 65536],
     "jet_fused_max_m": [1 << 16, 1 << 18, 1 << 20],
+    "jet_hub_deg": [256, 1024, 4096],
 }
 DEFAULTS = {"jet_graph_max_m": 1 << 24, "order_small_n": 16384, "match_coop_max_n": 1 << 17,
-            "match_coop_max_m": 1 << 21, "jet_fused_max_n": 8192, "jet_fused_max_m": 1 << 18}
+            "match_coop_max_m": 1 << 21, "jet_fused_max_n": 8192, "jet_fused_max_m": 1 << 18,
+            "jet_hub_deg": 1024}
 
 
 def _time(ctx, graphs, ks, config, seed, repeats):

@@ -132,6 +132,7 @@ struct Tunables {
     u64 match_coop_max_m = 1ull << 21; // ... and entries
     u32 jet_fused_max_n = 8192;        // whole Jet level loop in one block up to this many vertices ...
     u64 jet_fused_max_m = 1ull << 18;  // ... and entries
+    u32 jet_hub_deg = 1024;            // Jet table passes: rows above this length are cut into chunks of it (64..4096)
 };
 
 struct Ctx {

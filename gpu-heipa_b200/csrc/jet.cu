@@ -20,11 +20,12 @@ constexpr int JW_BLOCK = 128;      // 4 warps per block
 constexpr u32 JB_SLOTS = 16384;    // largest per-block table (128 KB)
 constexpr int JB_BLOCK = 512;
 constexpr u32 EMPTY = NO_BLOCK_ID;
-// Hub rows (more than JW_DEG entries) of the table-based passes are cut into
-// HUB_CHUNK-entry chunks, one warp each, when tables are direct-indexed and
+// Hub rows of the table-based passes are cut into chunks of hub_deg entries
+// (Tunables::jet_hub_deg), one warp each, when tables are direct-indexed and
 // k <= HUB_K; the chunks' partial connectivity is summed per row in global
-// memory and the last chunk to finish completes the row.
-constexpr u32 HUB_CHUNK = 4096;
+// memory and the last chunk to finish completes the row. With chunking
+// available, rows of more than hub_deg entries count as hubs, so that no warp
+// scans a long row alone.
 constexpr u32 HUB_K = 256;
 constexpr int ST_CHUNKS = 8;  // status slot: hub chunk items of the current pass
 constexpr u32 NOKEY = 0xFFFFFFFFu;
@@ -65,6 +66,7 @@ struct JArgs {
     s32 *hubacc;  // hub rows: k partial-connectivity sums per row slot (zero between uses), or null
     u32 *hubcnt;  // hub rows: finished chunks per row slot (zero between uses)
     u32 hub_cap;  // row slots of hubacc / hubcnt
+    u32 hub_deg;  // hub threshold and chunk length (entries) when hubacc is set
     s32 *abacc;  // afterburner partial sums of multi-chunk rows (zero between uses)
     u32 *abcnt;  // afterburner finished chunks of multi-chunk rows (zero between uses)
     DevStatus *st;
@@ -414,10 +416,10 @@ __device__ __forceinline__ void count_recompute(const JArgs &a, bool rec, u32 le
 }
 
 // Tier of a row for the table-based kernels: 0 thread, 1 warp, 2 block.
-__device__ __forceinline__ int table_tier(u32 len, u32 k) {
+__device__ __forceinline__ int table_tier(u32 len, u32 k, u32 warp_max = JW_DEG) {
     if (len <= JT) return 0;
     const u32 d = len < k ? len : k;
-    return (len <= JW_DEG && 2 * d <= JW_SLOTS) ? 1 : 2;
+    return (len <= warp_max && 2 * d <= JW_SLOTS) ? 1 : 2;
 }
 
 // Adds per-thread counts to the status word with one atomic per block.
@@ -485,7 +487,7 @@ __device__ __forceinline__ void chunk_range(const JArgs &a, unsigned long long i
 // emit nothing). Slots beyond the accumulator capacity are reported as an
 // error and skipped.
 __device__ __forceinline__ void emit_hub_chunks(const JArgs &a, u32 h, u32 len) {
-    u32 nch = len ? (len + HUB_CHUNK - 1) / HUB_CHUNK : 0u;
+    u32 nch = len ? (len + a.hub_deg - 1) / a.hub_deg : 0u;
     if (nch && h >= a.hub_cap) {
         set_error(&a.st->err, DEV_ERR_RANGE);
         nch = 0;
@@ -508,7 +510,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
                 const u32 len = a.g.rowlen[u];
                 ++nrec;
                 erec += len;
-                cls = table_tier(len, a.k);
+                cls = table_tier(len, a.k, a.hubacc ? a.hub_deg : JW_DEG);
                 if (cls == 0) lp_thread(a, u, ratio);
             }
         }
@@ -1045,7 +1047,7 @@ __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
                 if (!STRONG) a.dest_part[u] = o;
                 r.keys[u] = NOKEY;
             } else {
-                cls = table_tier(a.g.rowlen[u], a.k);
+                cls = table_tier(a.g.rowlen[u], a.k, a.hubacc ? a.hub_deg : JW_DEG);
                 if (cls == 0) rb_thread<STRONG>(a, r, u, o);
             }
         }
@@ -1114,9 +1116,9 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub(JArgs a, u32 ratio, RbArgs r) 
         const u32 h = (u32) (it >> 32);
         const u32 u = a.heavy2[h];
         const u32 len = __ldg(&a.g.rowlen[u]);
-        const u32 from = (u32) it * HUB_CHUNK;
-        const u32 to = len - from < HUB_CHUNK ? len : from + HUB_CHUNK;
-        const u32 nch = (len + HUB_CHUNK - 1) / HUB_CHUNK;
+        const u32 from = (u32) it * a.hub_deg;
+        const u32 to = len - from < a.hub_deg ? len : from + a.hub_deg;
+        const u32 nch = (len + a.hub_deg - 1) / a.hub_deg;
         dtable_build_range<false>(a, u, tv, from, to);
         s32 *acc = a.hubacc + (u64) h * a.k;
         for (u32 b = lane; b < a.k; b += 32) {
@@ -1895,6 +1897,7 @@ JArgs make_args(JetLevel &L) {
     a.hubacc = L.hubacc;
     a.hubcnt = L.hubcnt;
     a.hub_cap = L.hub_cap;
+    a.hub_deg = L.hub_deg;
     a.abcnt = L.abcnt;
     a.st = L.ctx->d_status;
     a.blk_slots = L.blk_slots;
@@ -2033,17 +2036,19 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     warp_direct = k <= JW_SLOTS && (d == nullptr || k <= 256);
     warp_slots = warp_direct ? k : JW_SLOTS;
     warp_smem = (JW_BLOCK / 32) * (warp_direct ? 1u : 2u) * warp_slots * (u32) sizeof(u32);
-    // chunk items (afterburner candidates, delta moves; each vertex at most
-    // once): one per row of <= CHUNK entries, so at most n + m / CHUNK + 1
-    items_cap = (u32) std::min<u64>(0xFFFFFFFFull, (u64) n + g.m / CHUNK + 1);
+    // chunk items (afterburner candidates, delta moves, hub chunks; each
+    // vertex at most once): one per row of <= CHUNK (hub_deg) entries, so at
+    // most n + m / min(CHUNK, hub_deg) + 1
+    hub_deg = std::min<u32>(JW_DEG, std::max<u32>(64, c.tune.jet_hub_deg));
+    items_cap = (u32) std::min<u64>(0xFFFFFFFFull, (u64) n + g.m / std::min<u32>(CHUNK, hub_deg) + 1);
     items = c.balloc<unsigned long long>(items_cap);
-    // hub-row accumulators (rows of more than JW_DEG entries: fewer than
-    // m / JW_DEG + 1 of them) when the tables are direct-indexed and k small
+    // hub-row accumulators (rows of more than hub_deg entries: fewer than
+    // m / hub_deg + 1 of them) when the tables are direct-indexed and k small
     hubacc = nullptr;
     hubcnt = nullptr;
     hub_cap = 0;
     if (warp_direct && k <= HUB_K) {
-        hub_cap = (u32) std::min<u64>(n, g.m / JW_DEG + 1);
+        hub_cap = (u32) std::min<u64>(n, g.m / hub_deg + 1);
         hubacc = c.balloc<s32>((u64) hub_cap * k);
         hubcnt = c.balloc<u32>(hub_cap);
         HP_CUDA(cudaMemsetAsync(hubacc, 0, sizeof(s32) * (u64) hub_cap * k, c.stream));

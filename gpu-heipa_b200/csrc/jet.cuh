@@ -67,6 +67,7 @@ struct JetLevel {
     s32 *hubacc = nullptr;  // hub-row connectivity accumulators (direct tables, small k), or null
     u32 *hubcnt = nullptr;  // hub-row finished-chunk counters
     u32 hub_cap = 0;        // hub-row slots
+    u32 hub_deg = 0;        // hub threshold and chunk length (entries)
     s32 *abacc = nullptr;  // afterburner partial sums of multi-chunk rows
     u32 *abcnt = nullptr;  // afterburner finished-chunk counts of multi-chunk rows
     u32 blk_slots = 0;  // block-tier table size

@@ -282,6 +282,7 @@ def test_direct_launch_paths_equal(ctx):
     try:
         for name in ("jet_graph_max_m", "order_small_n", "match_coop_max_n", "match_coop_max_m", "jet_fused_max_n"):
             c2.tune(name, 0)
+        c2.tune("jet_hub_deg", 4096)
         part, cut = c2.partition(g, 64, 0.03, "default", 7)
         assert cut == want_c
         np.testing.assert_array_equal(part, want_p)
