@@ -21,12 +21,17 @@ CANDIDATES = {
     "order_small_n": [0, 4096, 16384, 65536],
     "match_coop_max_n": [0, 1 << 15, 1 << 17, 1 << 19],
     "match_coop_max_m": [0, 1 << 19, 1 << 21, 1 << 23],
-    "jet_fused_max_n": [0, 2048, 8192, 32768, 65536],
+    "jet_fused_max_n": [0, 2048, 4096, 8192],
     "jet_fused_max_m": [1 << 16, 1 << 18, 1 << 20],
+    "jet_coop_max_n": [0, 16384, 65536],
+    "jet_coop_max_m": [1 << 19, 1 << 21, 1 << 23],
+    "jet_coop_max_deg": [16, 32, 64],
+    "jet_coop_rows": [512, 1024, 2048],
     "jet_hub_deg": [256, 1024, 4096],
 }
 DEFAULTS = {"jet_graph_max_m": 1 << 24, "order_small_n": 16384, "match_coop_max_n": 1 << 17,
-            "match_coop_max_m": 1 << 21, "jet_fused_max_n": 8192, "jet_fused_max_m": 1 << 18,
+            "match_coop_max_m": 1 << 21, "jet_fused_max_n": 4096, "jet_fused_max_m": 1 << 18,
+            "jet_coop_max_n": 65536, "jet_coop_max_m": 1 << 21, "jet_coop_max_deg": 32, "jet_coop_rows": 1024,
             "jet_hub_deg": 1024}
 
 

@@ -636,6 +636,10 @@ int hp_tune(hp_ctx *ctx, const char *name, int64_t value) {
     else if (nm == "match_coop_max_m") t.match_coop_max_m = (uint64_t) value;
     else if (nm == "jet_fused_max_n") t.jet_fused_max_n = (uint32_t) std::min<int64_t>(value, 0xFFFFFFFFll);
     else if (nm == "jet_fused_max_m") t.jet_fused_max_m = (uint64_t) value;
+    else if (nm == "jet_coop_max_n") t.jet_coop_max_n = (uint32_t) std::min<int64_t>(value, 0xFFFFFFFFll);
+    else if (nm == "jet_coop_max_m") t.jet_coop_max_m = (uint64_t) value;
+    else if (nm == "jet_coop_max_deg") t.jet_coop_max_deg = (uint32_t) std::min<int64_t>(value, 0xFFFFFFFFll);
+    else if (nm == "jet_coop_rows") t.jet_coop_rows = (uint32_t) std::min<int64_t>(value, 0xFFFFFFFFll);
     else if (nm == "jet_hub_deg") t.jet_hub_deg = (uint32_t) std::min<int64_t>(value, 0xFFFFFFFFll);
     else {
         ctx->c.last_error = "unknown tunable " + nm;

@@ -151,6 +151,44 @@ __device__ __forceinline__ u32 block_append(u32 *counter, bool pred, u32 *sm) {
 
 __device__ __forceinline__ void set_error(u32 *err, u32 bits) { atomicOr(err, bits); }
 
+// Grid-wide barrier for kernels launched with cudaLaunchCooperativeKernel
+// (all blocks resident), with a bounded wait. bar[0] counts arrivals and
+// bar[1] is the generation; both are zero before the launch. Thread 0 of each
+// block arrives and polls the generation at most GRID_BARRIER_SPINS times
+// (about a second); when that runs out it sets DEV_ERR_SPIN in *err. Returns
+// false in every thread of the block once *err carries DEV_ERR_SPIN, so the
+// caller leaves its loops; every later wait of the other blocks is bounded
+// too, so the kernel ends and the host reads the error.
+constexpr unsigned long long GRID_BARRIER_SPINS = 1ull << 24;
+
+__device__ __forceinline__ bool grid_barrier(u32 *bar, u32 *err) {
+    __shared__ u32 s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile u32 *vgen = bar + 1;
+        const u32 gen = *vgen;
+        __threadfence();
+        if (atomicAdd(&bar[0], 1u) == gridDim.x * gridDim.y * gridDim.z - 1) {
+            atomicExch(&bar[0], 0u);
+            __threadfence();
+            atomicAdd(&bar[1], 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*vgen == gen) {
+                if (++spins > GRID_BARRIER_SPINS) {
+                    set_error(err, DEV_ERR_SPIN);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = (*(volatile u32 *) err & DEV_ERR_SPIN) == 0u;
+    }
+    __syncthreads();
+    return s_ok != 0u;
+}
+
 // Number of kernels this process has launched (every launch site calls
 // note_launch()).
 extern std::atomic<unsigned long long> g_kernel_launches;

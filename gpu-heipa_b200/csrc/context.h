@@ -130,8 +130,12 @@ struct Tunables {
     u32 order_small_n = 16384;         // single-block rebalance ordering up to this many vertices
     u32 match_coop_max_n = 1u << 17;   // cooperative matching loop up to this many vertices ...
     u64 match_coop_max_m = 1ull << 21; // ... and entries
-    u32 jet_fused_max_n = 8192;        // whole Jet level loop in one block up to this many vertices ...
+    u32 jet_fused_max_n = 4096;        // whole Jet level loop in one block up to this many vertices ...
     u64 jet_fused_max_m = 1ull << 18;  // ... and entries
+    u32 jet_coop_max_n = 65536;        // ... else as a cooperative grid up to this many vertices ...
+    u64 jet_coop_max_m = 1ull << 21;   // ... and entries ...
+    u32 jet_coop_max_deg = 32;         // ... and average degree (dense levels keep the whole GPU)
+    u32 jet_coop_rows = 1024;          // vertices per block of that grid
     u32 jet_hub_deg = 1024;            // Jet table passes: rows above this length are cut into chunks of it (64..4096)
 };
 

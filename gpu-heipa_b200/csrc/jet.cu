@@ -1553,19 +1553,26 @@ __global__ void __launch_bounds__(OB, 1) k_order_small(JArgs a, RbArgs r, u32 wi
     order_small_body<STRONG>(a, r, width, key_bits, S, max_b_w, sm);
 }
 
-// ---- fused refinement of small levels -------------------------------------------------
+// ---- fused refinement of small and mid-size levels --------------------------------------
 
-// Levels of at most Tunables::jet_fused_max_n vertices run the whole level loop
-// of jet_refine in one 1024-thread block: the iteration control (ratios,
-// weak/strong switching, best-labelling tracking), and per iteration the same
-// steps as the per-kernel path (gain pass, filter, afterburner, weak or
-// strong rebalancing with the one-block ordering, perform). Everything stays
-// on one SM: counters and block weights live in shared memory, Jet state is
-// read with plain loads after __syncthreads(), so writes of earlier phases are
-// visible. The result equals the per-kernel path's (a parity test forces both).
-constexpr int FB = OB;                  // threads of the fused kernel (= the ordering block)
-constexpr u32 FUSED_MAX_N = 1u << 16;   // upper bound of Tunables::jet_fused_max_n
+// The whole level loop of jet_refine in one launch of 1024-thread blocks: the
+// iteration control (ratios, weak/strong switching, best-labelling tracking)
+// and per iteration the same steps as the per-kernel path (gain pass, filter,
+// afterburner, weak or strong rebalancing with the one-block ordering,
+// perform). Levels of at most Tunables::jet_fused_max_n vertices run it in a
+// single block (phases separated by __syncthreads()); levels of at most
+// Tunables::jet_coop_max_n vertices run it as a cooperative grid (phases
+// separated by grid barriers; block 0 alone does the ordering). State written
+// in one phase is read in a later phase with plain loads after the barrier
+// (never through the non-coherent path). Every branch of the control flow
+// depends only on values all threads read after the same barrier, so every
+// thread reaches every barrier. The result equals the per-kernel path's (a
+// parity test forces both).
+constexpr int FB = OB;                  // threads per block (= the ordering block)
+constexpr u32 FUSED_MAX_N = 1u << 16;   // upper bound of both vertex thresholds (one-block ordering)
 constexpr u32 FUSED_AB_THREAD = 32;     // afterburner / delta rows handled by one thread
+constexpr int FC_N = 4;  // counters per set: warp rows, block rows, candidates, moves
+constexpr int FS_N = 2;  // sums per set: moved-row entries, objective delta
 
 struct FusedCtl {
     u32 n_ratios;
@@ -1582,15 +1589,28 @@ struct FusedArgs {
     u32 width;
     int bits_weak, bits_strong;
     OrderScratch S;
-    u32 *under; // writable alias of weak.under
-    u32 *part;  // receives the best labelling
+    u32 *under;       // writable alias of weak.under
+    u32 *part;        // receives the best labelling
+    u32 *gcnt;        // cooperative grid: 2 sets of FC_N counters (zero on entry)
+    long long *gsum;  // cooperative grid: 2 sets of FS_N sums (zero on entry)
+    u32 *bar;         // cooperative grid: barrier words (zero on entry)
 };
 
-// Block weights kept in shared memory during the fused kernel and mirrored to
-// a.bw (plain stores) for the functions that read it.
-__device__ __forceinline__ void fused_publish_bw(const JArgs &a, const s32 *sbw) {
-    for (u32 b = threadIdx.x; b < a.k; b += blockDim.x) a.bw[b] = sbw[b];
+// Barrier of the team: the block, or the cooperative grid (bounded wait;
+// false once a wait gave up).
+template<bool COOP>
+__device__ __forceinline__ bool team_sync(u32 *bar, u32 *err) {
+    if (COOP) return grid_barrier(bar, err);
     __syncthreads();
+    return true;
+}
+
+// Loads a value that decides the control flow (counts, sums, block weights)
+// after a barrier: from L2 on a grid (global memory), a volatile load within
+// one block (shared or global memory), so every thread sees the same value.
+template<bool COOP, typename T>
+__device__ __forceinline__ T ld_team(const T *p) {
+    return COOP ? __ldcg(p) : *(const volatile T *) p;
 }
 
 __device__ __forceinline__ long long block_sum_ll(long long v, long long *sm) {
@@ -1608,243 +1628,314 @@ __device__ __forceinline__ long long block_sum_ll(long long v, long long *sm) {
     return r;
 }
 
-__global__ void __launch_bounds__(FB, 1) k_jet_fused(JArgs a, FusedArgs F, FusedCtl *ctl) {
+// Adds v over all threads into *slot (zero beforehand), synchronises the team
+// and reads the total into out; false once a barrier wait gave up.
+template<bool COOP>
+__device__ __forceinline__ bool team_sum(long long v, long long *slot, long long *sm, u32 *bar, u32 *err,
+                                         long long &out) {
+    v = block_sum_ll(v, sm);
+    if (threadIdx.x == 0 && v) atomicAdd((unsigned long long *) slot, (unsigned long long) v);
+    if (!team_sync<COOP>(bar, err)) return false;
+    out = ld_team<COOP>(slot);
+    return true;
+}
+
+#define TEAM_SYNC()                                          \
+    do {                                                     \
+        if (!team_sync<COOP>(F.bar, &a.st->err)) goto finish; \
+    } while (0)
+
+template<bool COOP>
+__global__ void __launch_bounds__(FB, 1) k_jet_loop(JArgs a, FusedArgs F, FusedCtl *ctl) {
     extern __shared__ s32 fsm[];
-    s32 *wtab = fsm + (u32) warp_in_block() * a.k;  // per-warp direct table
-    s32 *btab = fsm + 32u * a.k;                    // block table
-    s32 *sbw = fsm + 33u * a.k;                     // block weights
-    __shared__ u32 sc[8];
+    const u32 tid = threadIdx.x, lane = lane_id(), warp = warp_in_block(), n = a.g.n, k = a.k;
+    s32 *wtab = fsm + warp * k;  // per-warp direct table
+    s32 *btab = fsm + 32u * k;   // block table
+    s32 *sbd = fsm + 33u * k;    // block-weight changes of this block's moves
+    __shared__ u32 scnt[2 * FC_N];
+    __shared__ long long ssum[2 * FS_N];
     __shared__ long long sl[33];
     __shared__ unsigned long long smu[33];
     __shared__ long long sms[33];
-    __shared__ int si[2];
+    __shared__ s32 smx[32];
     __shared__ OrderSmem osm;
-    const u32 tid = threadIdx.x, lane = lane_id(), warp = warp_in_block(), n = a.g.n, k = a.k;
-    for (u32 i = tid; i < 33u * k; i += FB) fsm[i] = 0;
-    for (u32 b = tid; b < k; b += FB) sbw[b] = a.bw[b];
+    for (u32 i = tid; i < 34u * k; i += FB) fsm[i] = 0;
+    if (!COOP && tid < 2 * FC_N) scnt[tid] = 0;
+    if (!COOP && tid < 2 * FS_N) ssum[tid] = 0;
     __syncthreads();
+    u32 *const cnt_base = COOP ? F.gcnt : scnt;
+    long long *const sum_base = COOP ? F.gsum : ssum;
+    const u32 nthreads = gridDim.x * FB;
+    const u32 wbase0 = blockIdx.x * FB + warp * 32u;  // first row of this warp in grid-stride loops
+    const u32 gwarps = gridDim.x * (FB / 32), gw = blockIdx.x * (FB / 32) + warp;
     const ConnTable<false, true, false> WT{nullptr, wtab, 0, k};
     const ConnTable<true, true, false> BT{nullptr, btab, 0, k};
     const bool promap = ctl->promap != 0;
     const s32 lmax = ctl->lmax;
+    const u32 n_ratios = ctl->n_ratios;
     long long obj = ctl->obj, best_obj = obj;
     s32 maxw = ctl->maxw, best_max = maxw;
-    u32 iterations = 0;
-    for (u32 ri = 0; ri < ctl->n_ratios; ++ri) {
+    u32 iterations = 0, it = 0;
+    for (u32 ri = 0; ri < n_ratios; ++ri) {
         const u32 ratio = ctl->ratios[ri];
         u32 balance_iteration = 0, iteration = 0;
         while (iteration < JET_MAX_ITERATIONS) {
             iteration += 1;
             ++iterations;
+            // counter set of this iteration (zero); the other set is cleared
+            // after the first barrier, when every thread is done reading it
+            const u32 set = it & 1u;
+            ++it;
+            u32 *const cnt = cnt_base + set * FC_N;
+            long long *const sum = sum_base + set * FS_N;
+            const bool clears = blockIdx.x == 0 && tid < (u32) FC_N;
             bool lp_iter = false;
             int step;
-            if (!promap) {
-                if (maxw <= lmax) {
-                    step = 0;
-                    lp_iter = true;
-                    balance_iteration = 0;
-                } else {
-                    step = balance_iteration < JET_MAX_WEAK_ITERATIONS ? 1 : 2;
-                }
+            if (maxw <= lmax) {
+                step = 0;
+                lp_iter = true;
+                balance_iteration = 0;
+            } else if (!promap) {
+                step = balance_iteration < JET_MAX_WEAK_ITERATIONS ? 1 : 2;
             } else {
-                if (maxw <= lmax) {
-                    step = 0;
-                    lp_iter = true;
-                    balance_iteration = 0;
-                } else {
-                    balance_iteration++;
-                    step = balance_iteration < JET_MAX_WEAK_ITERATIONS ? 1 : 2;
-                }
+                balance_iteration++;
+                step = balance_iteration < JET_MAX_WEAK_ITERATIONS ? 1 : 2;
             }
-            if (tid < 8) sc[tid] = 0;
-            __syncthreads();
+            u32 nm;
             if (step == 0) {
                 // gain pass (jet_lp :193-238): cached targets, else recompute
-                for (u32 u = tid; u < n; u += FB) {
-                    const u32 dc = a.dest_cache[u];
-                    if (dc != NULL_PART) {
-                        a.dest_part[u] = dc;
-                        continue;
-                    }
-                    const int cls = table_tier(a.g.rowlen[u], k);
-                    if (cls == 0) lp_thread<false>(a, u, ratio);
-                    else if (cls == 1) a.heavy[atomicAdd(&sc[0], 1u)] = u;
-                    else a.heavy2[atomicAdd(&sc[1], 1u)] = u;
-                }
-                __syncthreads();
-                for (u32 i = warp; i < sc[0]; i += FB / 32) lp_group<false, true, false>(a, a.heavy[i], ratio, WT, nullptr, nullptr);
-                __syncthreads();
-                for (u32 i = 0; i < sc[1]; ++i) lp_group<true, true, false>(a, a.heavy2[i], ratio, BT, smu, sms);
-                __syncthreads();
-                // filter (:247-258)
-                for (u32 u = tid; u < n; u += FB) {
-                    if (a.dest_part[u] != NO_MOVE && a.lock[u] == 0) {
-                        a.gain1[u] = a.gain_cache[u];
-                        a.cand[atomicAdd(&sc[2], 1u)] = u;
-                    } else {
-                        a.gain1[u] = GAIN_MIN;
-                        a.lock[u] = 0;
-                    }
-                }
-                __syncthreads();
-                // afterburner: short rows by a thread, longer ones by a warp
-                const u32 nc = sc[2];
-                for (u32 i = tid; i < nc; i += FB) {
-                    const u32 u = a.cand[i];
-                    const u32 len = a.g.rowlen[u];
-                    if (len <= FUSED_AB_THREAD) {
-                        const s32 ug = a.gain1[u];
-                        if (wadd(ug, ab_range<false>(a, u, ug, a.map[u], a.dest_part[u], 0, len, 0, 1)) >= 0) {
-                            a.lock[u] = 1;
-                            a.moves[atomicAdd(&sc[3], 1u)] = u;
+                for (u32 wb = wbase0; wb < n; wb += nthreads) {
+                    const u32 u = wb + lane;
+                    int cls = -1;
+                    if (u < n) {
+                        const u32 dc = a.dest_cache[u];
+                        if (dc != NULL_PART) {
+                            a.dest_part[u] = dc;
+                        } else {
+                            cls = table_tier(a.g.rowlen[u], k);
+                            if (cls == 0) lp_thread<false>(a, u, ratio);
                         }
-                    } else {
-                        a.heavy[atomicAdd(&sc[4], 1u)] = u;
                     }
+                    const u32 s1 = warp_append(&cnt[0], cls == 1);
+                    if (cls == 1) a.heavy[s1] = u;
+                    const u32 s2 = warp_append(&cnt[1], cls == 2);
+                    if (cls == 2) a.heavy2[s2] = u;
                 }
-                __syncthreads();
-                for (u32 i = warp; i < sc[4]; i += FB / 32) {
-                    const u32 u = a.heavy[i];
-                    const s32 ug = a.gain1[u];
-                    const s32 change = (s32) warp_sum<u32>(
-                        (u32) ab_range<false>(a, u, ug, a.map[u], a.dest_part[u], 0, a.g.rowlen[u], lane, 32));
-                    if (lane == 0 && wadd(ug, change) >= 0) {
-                        a.lock[u] = 1;
-                        a.moves[atomicAdd(&sc[3], 1u)] = u;
+                TEAM_SYNC();
+                if (clears) cnt_base[(set ^ 1u) * FC_N + tid] = 0;
+                if (clears && tid < (u32) FS_N) sum_base[(set ^ 1u) * FS_N + tid] = 0;
+                const u32 n1 = ld_team<COOP>(&cnt[0]), n2 = ld_team<COOP>(&cnt[1]);
+                for (u32 i = gw; i < n1; i += gwarps) lp_group<false, true, false>(a, a.heavy[i], ratio, WT, nullptr, nullptr);
+                for (u32 i = blockIdx.x; i < n2; i += gridDim.x) lp_group<true, true, false>(a, a.heavy2[i], ratio, BT, smu, sms);
+                TEAM_SYNC();
+                // filter (:247-258)
+                for (u32 wb = wbase0; wb < n; wb += nthreads) {
+                    const u32 u = wb + lane;
+                    bool c = false;
+                    if (u < n) {
+                        c = a.dest_part[u] != NO_MOVE && a.lock[u] == 0;
+                        if (c) {
+                            a.gain1[u] = a.gain_cache[u];
+                        } else {
+                            a.gain1[u] = GAIN_MIN;
+                            a.lock[u] = 0;
+                        }
                     }
+                    const u32 s3 = warp_append(&cnt[2], c);
+                    if (c) a.cand[s3] = u;
                 }
-                __syncthreads();
-                if (tid == 0) a.st->cnt[ST_MOVES] = sc[3];
-                __syncthreads();
+                TEAM_SYNC();
+                // afterburner: short rows by a thread, longer ones by the whole warp
+                const u32 nc = ld_team<COOP>(&cnt[2]);
+                for (u32 wb = wbase0; wb < nc; wb += nthreads) {
+                    const u32 i = wb + lane;
+                    u32 u = 0, len = 0;
+                    bool lock = false;
+                    if (i < nc) {
+                        u = a.cand[i];
+                        len = a.g.rowlen[u];
+                        if (len <= FUSED_AB_THREAD) {
+                            const s32 ug = a.gain1[u];
+                            lock = wadd(ug, ab_range<false>(a, u, ug, a.map[u], a.dest_part[u], 0, len, 0, 1)) >= 0;
+                        }
+                    }
+                    unsigned longer = __ballot_sync(FULL, i < nc && len > FUSED_AB_THREAD);
+                    while (longer) {
+                        const int src = __ffs(longer) - 1;
+                        longer &= longer - 1;
+                        const u32 v = __shfl_sync(FULL, u, src), lv = __shfl_sync(FULL, len, src);
+                        const s32 vg = a.gain1[v];
+                        const s32 change = (s32) warp_sum<u32>(
+                            (u32) ab_range<false>(a, v, vg, a.map[v], a.dest_part[v], 0, lv, lane, 32));
+                        if (lane == (u32) src) lock = wadd(vg, change) >= 0;
+                    }
+                    if (lock) a.lock[u] = 1;
+                    const u32 s4 = warp_append(&cnt[3], lock);
+                    if (lock) a.moves[s4] = u;
+                }
+                TEAM_SYNC();
+                nm = ld_team<COOP>(&cnt[3]);
             } else {
                 // rebalancing picks (rebalance_weak :592-751 / rebalance_strong :356-590)
                 const bool strong = step == 2;
                 const RbArgs &r = strong ? F.strong : F.weak;
-                if (strong) maxv_block(a.bw, k, r.max_b_w, &a.st->imax[1]);
-                else under_block(a.bw, k, r.max_b_w, F.under, &a.st->cnt[ST_AUX]);
-                __syncthreads();
-                const s32 maxv = a.st->imax[1];
-                for (u32 u = tid; u < n; u += FB) {
-                    const u32 o = a.map[u];
-                    const bool q = strong ? rb_qualifies<true>(a, r, o, g_vw(a.g, u), maxv)
-                                          : rb_qualifies<false>(a, r, o, g_vw(a.g, u), maxv);
-                    if (!q) {
-                        if (!strong) a.dest_part[u] = o;
-                        r.keys[u] = NOKEY;
-                        continue;
-                    }
-                    const int cls = table_tier(a.g.rowlen[u], k);
-                    if (cls == 0) {
-                        if (strong) rb_thread<true, false>(a, r, u, o);
-                        else rb_thread<false, false>(a, r, u, o);
-                    } else if (cls == 1) {
-                        a.heavy[atomicAdd(&sc[0], 1u)] = u;
-                    } else {
-                        a.heavy2[atomicAdd(&sc[1], 1u)] = u;
-                    }
+                if (blockIdx.x == 0) {
+                    if (strong) maxv_block(a.bw, k, r.max_b_w, &a.st->imax[1]);
+                    else under_block(a.bw, k, r.max_b_w, F.under, &a.st->cnt[ST_AUX]);
                 }
-                __syncthreads();
-                for (u32 i = warp; i < sc[0]; i += FB / 32) {
+                TEAM_SYNC();
+                if (clears) cnt_base[(set ^ 1u) * FC_N + tid] = 0;
+                if (clears && tid < (u32) FS_N) sum_base[(set ^ 1u) * FS_N + tid] = 0;
+                const s32 maxv = ld_team<COOP>(&a.st->imax[1]);
+                for (u32 wb = wbase0; wb < n; wb += nthreads) {
+                    const u32 u = wb + lane;
+                    int cls = -1;
+                    if (u < n) {
+                        const u32 o = a.map[u];
+                        const bool q = strong ? rb_qualifies<true>(a, r, o, g_vw(a.g, u), maxv)
+                                              : rb_qualifies<false>(a, r, o, g_vw(a.g, u), maxv);
+                        if (!q) {
+                            if (!strong) a.dest_part[u] = o;
+                            r.keys[u] = NOKEY;
+                        } else {
+                            cls = table_tier(a.g.rowlen[u], k);
+                            if (cls == 0) {
+                                if (strong) rb_thread<true, false>(a, r, u, o);
+                                else rb_thread<false, false>(a, r, u, o);
+                            }
+                        }
+                    }
+                    const u32 s1 = warp_append(&cnt[0], cls == 1);
+                    if (cls == 1) a.heavy[s1] = u;
+                    const u32 s2 = warp_append(&cnt[1], cls == 2);
+                    if (cls == 2) a.heavy2[s2] = u;
+                }
+                TEAM_SYNC();
+                const u32 n1 = ld_team<COOP>(&cnt[0]), n2 = ld_team<COOP>(&cnt[1]);
+                for (u32 i = gw; i < n1; i += gwarps) {
                     if (strong) rb_group<true, false, true, false>(a, r, a.heavy[i], WT, nullptr, nullptr);
                     else rb_group<false, false, true, false>(a, r, a.heavy[i], WT, nullptr, nullptr);
                 }
-                __syncthreads();
-                for (u32 i = 0; i < sc[1]; ++i) {
+                for (u32 i = blockIdx.x; i < n2; i += gridDim.x) {
                     if (strong) rb_group<true, true, true, false>(a, r, a.heavy2[i], BT, smu, sms);
                     else rb_group<false, true, true, false>(a, r, a.heavy2[i], BT, smu, sms);
                 }
-                __syncthreads();
-                if (strong) order_small_body<true>(a, r, F.width, F.bits_strong, F.S, r.max_b_w, osm);
-                else order_small_body<false>(a, r, F.width, F.bits_weak, F.S, r.max_b_w, osm);
-                __syncthreads();
+                TEAM_SYNC();
+                if (blockIdx.x == 0) {
+                    if (strong) order_small_body<true>(a, r, F.width, F.bits_strong, F.S, r.max_b_w, osm);
+                    else order_small_body<false>(a, r, F.width, F.bits_weak, F.S, r.max_b_w, osm);
+                }
+                TEAM_SYNC();
+                nm = ld_team<COOP>(&a.st->cnt[ST_MOVES]);
             }
-            const u32 nm = a.st->cnt[ST_MOVES];
             // perform_moves (:753-924): labels with the moved bit, block weights
             long long entries = 0;
-            for (u32 i = tid; i < nm; i += FB) {
+            for (u32 i = blockIdx.x * FB + tid; i < nm; i += nthreads) {
                 const u32 u = a.moves[i];
                 const u32 ou = a.map[u], nu = a.dest_part[u];
                 const s32 w = g_vw(a.g, u);
                 if (ou != nu) {
-                    atomicSub(&sbw[ou], w);
-                    atomicAdd(&sbw[nu], w);
+                    atomicSub(&sbd[ou], w);
+                    atomicAdd(&sbd[nu], w);
                 }
                 a.map[u] = ou != nu ? (nu | MOVED) : nu;
                 a.dest_part[u] = ou;
                 a.dest_cache[u] = NULL_PART;
                 entries += a.g.rowlen[u];
             }
-            entries = block_sum_ll(entries, sl);
+            __syncthreads();
+            for (u32 b = tid; b < k; b += FB)
+                if (sbd[b]) {
+                    atomicAdd(&a.bw[b], sbd[b]);
+                    sbd[b] = 0;
+                }
+            long long ent = 0;
+            if (!team_sum<COOP>(entries, &sum[0], sl, F.bar, &a.st->err, ent)) goto finish;
+            const bool inval = (unsigned long long) ent < a.inval_all_min;
             s32 m = 0;
-            for (u32 b = tid; b < k; b += FB) m = sbw[b] > m ? sbw[b] : m;
-            m = __reduce_max_sync(FULL, m);
-            if (lane == 0) sl[warp] = m;
-            __syncthreads();
-            if (tid == 0) {
-                s32 r = 0;
-                for (u32 w = 0; w < FB / 32; ++w) r = (s32) sl[w] > r ? (s32) sl[w] : r;
-                si[0] = r;
+            for (u32 b = tid; b < k; b += FB) {
+                const s32 x = ld_team<COOP>(&a.bw[b]);
+                m = x > m ? x : m;
             }
+            m = __reduce_max_sync(FULL, m);
+            if (lane == 0) smx[warp] = m;
             __syncthreads();
-            const s32 new_maxw = si[0];
-            const bool inval = (unsigned long long) entries < a.inval_all_min;
+            s32 new_maxw = 0;
+            for (u32 w = 0; w < FB / 32; ++w) new_maxw = smx[w] > new_maxw ? smx[w] : new_maxw;
             // exact objective change and the neighbours' cache resets
             long long acc = 0;
-            for (u32 i = tid; i < nm; i += FB) {
-                const u32 u = a.moves[i];
-                const u32 len = a.g.rowlen[u];
-                if (len <= FUSED_AB_THREAD) acc += delta_range<false>(a, u, 0, len, 0, 1, inval);
-                else a.heavy[atomicAdd(&sc[5], 1u)] = u;
+            for (u32 wb = wbase0; wb < nm; wb += nthreads) {
+                const u32 i = wb + lane;
+                u32 u = 0, len = 0;
+                if (i < nm) {
+                    u = a.moves[i];
+                    len = a.g.rowlen[u];
+                    if (len <= FUSED_AB_THREAD) acc += delta_range<false>(a, u, 0, len, 0, 1, inval);
+                }
+                unsigned longer = __ballot_sync(FULL, i < nm && len > FUSED_AB_THREAD);
+                while (longer) {
+                    const int src = __ffs(longer) - 1;
+                    longer &= longer - 1;
+                    const u32 v = __shfl_sync(FULL, u, src), lv = __shfl_sync(FULL, len, src);
+                    acc += delta_range<false>(a, v, 0, lv, lane, 32, inval);
+                }
             }
-            __syncthreads();
-            for (u32 i = warp; i < sc[5]; i += FB / 32) {
-                const u32 u = a.heavy[i];
-                acc += delta_range<false>(a, u, 0, a.g.rowlen[u], lane, 32, inval);
-            }
-            const long long d = block_sum_ll(acc, sl);
+            long long d = 0;
+            if (!team_sum<COOP>(acc, &sum[1], sl, F.bar, &a.st->err, d)) goto finish;
             if (!inval)
-                for (u32 u = tid; u < n; u += FB) a.dest_cache[u] = NULL_PART;
-            for (u32 i = tid; i < nm; i += FB) a.map[a.moves[i]] &= ~MOVED;
-            fused_publish_bw(a, sbw);  // includes __syncthreads()
-            // control (jet_label_propagation.h:966-1030, promap :1250-1305)
+                for (u32 u = blockIdx.x * FB + tid; u < n; u += nthreads) a.dest_cache[u] = NULL_PART;
+            for (u32 i = blockIdx.x * FB + tid; i < nm; i += nthreads) a.map[a.moves[i]] &= ~MOVED;
+            // control (jet_label_propagation.h:966-1030, promap :1250-1305):
+            // 1 = next iteration, 2 = next ratio
+            int action = 0;
             if (!promap) {
                 if (nm == 0) {
-                    if (lp_iter) break;
-                    if (balance_iteration < JET_MAX_WEAK_ITERATIONS) {
+                    if (lp_iter) {
+                        action = 2;
+                    } else if (balance_iteration < JET_MAX_WEAK_ITERATIONS) {
                         balance_iteration = JET_MAX_WEAK_ITERATIONS;
-                        continue;
+                        action = 1;
+                    } else {
+                        action = 2;
                     }
-                    break;
+                } else if (!lp_iter) {
+                    balance_iteration++;
                 }
-                if (!lp_iter) balance_iteration++;
             } else if (nm == 0) {
-                continue;
+                action = 1;
             }
-            obj += promap ? d : d / 2;
-            maxw = new_maxw;
-            const bool leq = promap ? (maxw < best_max) : (maxw <= best_max);
             bool copy = false;
-            if (best_max > lmax && maxw < best_max) {
-                copy = true;
-                iteration = 0;
-            } else if (obj < best_obj && (maxw <= lmax || leq)) {
-                if (1000 * obj < 999 * best_obj) iteration = 0;  // PHI = 0.999
-                copy = true;
+            if (action == 0) {
+                obj += promap ? d : d / 2;
+                maxw = new_maxw;
+                const bool leq = promap ? (maxw < best_max) : (maxw <= best_max);
+                if (best_max > lmax && maxw < best_max) {
+                    copy = true;
+                    iteration = 0;
+                } else if (obj < best_obj && (maxw <= lmax || leq)) {
+                    if (1000 * obj < 999 * best_obj) iteration = 0;  // PHI = 0.999
+                    copy = true;
+                }
+                if (copy) {
+                    best_obj = obj;
+                    best_max = maxw;
+                }
             }
-            if (copy) {
-                for (u32 u = tid; u < n; u += FB) F.part[u] = a.map[u];
-                best_obj = obj;
-                best_max = maxw;
-                __syncthreads();
-            }
+            if (copy)  // the moved bits may still be set here: mask them
+                for (u32 u = blockIdx.x * FB + tid; u < n; u += nthreads) F.part[u] = a.map[u] & ~MOVED;
+            TEAM_SYNC();
+            if (action == 2) break;
         }
     }
-    if (tid == 0) {
+    if (blockIdx.x == 0 && tid == 0) {
         ctl->obj = best_obj;
         ctl->maxw = best_max;
         ctl->iterations = iterations;
     }
+finish:;
 }
+
+#undef TEAM_SYNC
 
 // ---- objectives ------------------------------------------------------------------
 
@@ -1929,7 +2020,9 @@ void set_big_smem() {
     HP_CUDA(cudaFuncSetAttribute(k_lp_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     HP_CUDA(cudaFuncSetAttribute(k_rb_block<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     HP_CUDA(cudaFuncSetAttribute(k_rb_block<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    HP_CUDA(cudaFuncSetAttribute(k_jet_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    HP_CUDA(cudaFuncSetAttribute(k_jet_loop<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) (34 * JW_SLOTS * sizeof(s32))));
+    HP_CUDA(cudaFuncSetAttribute(k_jet_loop<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int) (34 * JW_SLOTS * sizeof(s32))));
     done.push_back(dev);
 }
@@ -2405,10 +2498,11 @@ void JetLevel::run_step(int kind, u32 ratio_pct) {
     c.sync();
 }
 
-// The whole level loop in one k_jet_fused launch (warp_direct levels of at
-// most FUSED_MAX_N vertices); writes the best labelling to part.
+// The whole level loop in one k_jet_loop launch (warp_direct levels of at
+// most FUSED_MAX_N vertices): one block, or a cooperative grid of `blocks`
+// blocks; writes the best labelling to part.
 static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &ratios, bool promap, u32 *part,
-                             s64 &obj, s32 &maxw) {
+                             s64 &obj, s32 &maxw, u32 blocks) {
     const u32 n = L.g.n, k = L.k;
     const s32 opt = (L.g_weight + (s32) (k - 1)) / (s32) k;
     u32 sections, width;
@@ -2437,6 +2531,12 @@ static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &rati
     S.fail = ctx.balloc<u32>(n);
     S.fail2 = ctx.balloc<u32>(n);
     F.part = part;
+    F.gcnt = ctx.balloc<u32>(2 * FC_N);
+    F.gsum = ctx.balloc<long long>(2 * FS_N);
+    F.bar = ctx.balloc<u32>(2);
+    HP_CUDA(cudaMemsetAsync(F.bar, 0, 2 * sizeof(u32), ctx.stream));
+    HP_CUDA(cudaMemsetAsync(F.gcnt, 0, 2 * FC_N * sizeof(u32), ctx.stream));
+    HP_CUDA(cudaMemsetAsync(F.gsum, 0, 2 * FS_N * sizeof(long long), ctx.stream));
     FusedCtl h{};
     h.n_ratios = (u32) ratios.size();
     for (size_t i = 0; i < ratios.size() && i < 17; ++i) h.ratios[i] = ratios[i];
@@ -2447,16 +2547,38 @@ static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &rati
     FusedCtl *d = ctx.balloc<FusedCtl>(1);
     HP_CUDA(cudaMemcpyAsync(d, &h, sizeof(FusedCtl), cudaMemcpyHostToDevice, ctx.stream));
     ctx.zero_counters();
-    {
+    const size_t smem = 34 * (size_t) k * sizeof(s32);
+    JArgs a = make_args(L);
+    if (blocks <= 1) {
         KernTimer kt(ctx, "k_jet_fused");
-        k_jet_fused<<<1, FB, 34 * k * sizeof(s32), ctx.stream>>>(make_args(L), F, d); note_launch();
+        k_jet_loop<false><<<1, FB, smem, ctx.stream>>>(a, F, d); note_launch();
+    } else {
+        KernTimer kt(ctx, "k_jet_coop");
+        void *args[] = {&a, &F, &d};
+        HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_jet_loop<true>, dim3(blocks), dim3(FB), args, smem,
+                                            ctx.stream));
+        note_launch();
     }
     HP_LAUNCH_CHECK();
     HP_CUDA(cudaMemcpyAsync(&h, d, sizeof(FusedCtl), cudaMemcpyDeviceToHost, ctx.stream));
     const DevStatus &st = ctx.read_status();
+    if (st.err & DEV_ERR_SPIN) throw HpError{HP_ERR_DEVICE, "Jet level loop: a grid barrier wait gave up"};
     if (st.err) throw HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
     obj = h.obj;
     maxw = h.maxw;
+}
+
+// Blocks of the cooperative level loop for a level of n vertices (0 when it
+// does not apply): one per Tunables::jet_coop_rows vertices, at least two, at
+// most as many as fit on the GPU at once.
+static u32 coop_blocks(Ctx &ctx, u32 n, u32 k) {
+    int per_sm = 0;
+    HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jet_loop<true>, FB,
+                                                          34 * (size_t) k * sizeof(s32)));
+    if (per_sm <= 0) return 0;
+    const u64 rows = std::max<u32>(1, ctx.tune.jet_coop_rows);
+    const u64 want = ((u64) n + rows - 1) / rows;
+    return (u32) std::max<u64>(2, std::min<u64>(want, (u64) per_sm * ctx.sm_count));
 }
 
 void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultra, u32 level, s64 &obj, s32 &maxw,
@@ -2475,10 +2597,20 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
     std::vector<u32> ratios;
     if (ultra && !promap) ratios = {85, 80, 75, 70, 65, 60, 55, 50, 45, 40, 35, 30, 25, 20, 15, 10, 5};
     else ratios = {level == 0 ? 25u : 75u};
-    if (L.warp_direct && g.n <= std::min<u32>(ctx.tune.jet_fused_max_n, FUSED_MAX_N) &&
-        g.m <= ctx.tune.jet_fused_max_m && !ctx.prof.enabled) {
-        jet_refine_fused(ctx, L, ratios, promap, part, obj, maxw);
-        return;
+    if (L.warp_direct && !ctx.prof.enabled) {
+        if (g.n <= std::min<u32>(ctx.tune.jet_fused_max_n, FUSED_MAX_N) && g.m <= ctx.tune.jet_fused_max_m) {
+            jet_refine_fused(ctx, L, ratios, promap, part, obj, maxw, 1);
+            return;
+        }
+        if (g.n <= std::min<u32>(ctx.tune.jet_coop_max_n, FUSED_MAX_N) && g.m <= ctx.tune.jet_coop_max_m &&
+            g.m <= (u64) ctx.tune.jet_coop_max_deg * g.n) {
+            set_big_smem();
+            const u32 blocks = coop_blocks(ctx, g.n, k);
+            if (blocks) {
+                jet_refine_fused(ctx, L, ratios, promap, part, obj, maxw, blocks);
+                return;
+            }
+        }
     }
     for (u32 ratio: ratios) {
         u32 balance_iteration = 0, iteration = 0;

@@ -4,9 +4,7 @@
 #include "coarsen.cuh"
 #include "prims.cuh"
 
-#include <cooperative_groups.h>
 
-namespace cg = cooperative_groups;
 
 namespace hp {
 namespace {
@@ -288,8 +286,7 @@ constexpr u32 MATCH_COOP_MAX_N = 1u << 20;
 
 __global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap, u32 *hn, u32 *list, u32 *list2,
                                                            u32 cnt, unsigned long long *claim, u32 *heavy, u32 *huge,
-                                                           u32 *ctr, u32 seed) {
-    cg::grid_group grid = cg::this_grid();
+                                                           u32 *ctr, u32 seed, u32 *bar, u32 *err) {
     __shared__ PickLocal sm[32];
     const u64 gtid = (u64) blockIdx.x * blockDim.x + threadIdx.x;
     const u64 gsize = (u64) gridDim.x * blockDim.x;
@@ -314,7 +311,7 @@ __global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap,
             if (v == SENTINEL || __ldcg(&vcmap[u]) != SENTINEL) continue;
             if (!commit_cond(u, v, 0)) vcmap[u] = SENTINEL - 1;
         }
-        grid.sync();
+        if (!grid_barrier(bar, err)) return;
         for (u32 r = 0; r < 4; ++r) {
             ++epoch;
             const u32 tag = 0xFFFFFFFFu - epoch;
@@ -324,7 +321,7 @@ __global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap,
                 if (v == SENTINEL || __ldcg(&vcmap[u]) != SENTINEL) continue;
                 if (__ldcg(&vcmap[v]) == SENTINEL - 1) atomicMin(&claim[v], ((unsigned long long) tag << 32) | u);
             }
-            grid.sync();
+            if (!grid_barrier(bar, err)) return;
             const int next_r = r < 3 ? (int) r + 1 : -1;
             for (u64 i = gtid; i < cnt; i += gsize) {
                 const u32 u = list[i];
@@ -341,7 +338,7 @@ __global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap,
                     st = SENTINEL - 1;
                 vcmap[u] = st;
             }
-            grid.sync();
+            if (!grid_barrier(bar, err)) return;
         }
         // re-pick for vertices whose target got matched
         for (u64 base = (u64) blockIdx.x * blockDim.x; base < cnt; base += gsize) {
@@ -358,7 +355,7 @@ __global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap,
             }
             append_tier(tier, u, heavy, &ctr[1], huge, &ctr[2]);
         }
-        grid.sync();
+        if (!grid_barrier(bar, err)) return;
         const u32 nh = __ldcg(&ctr[1]), ng = __ldcg(&ctr[2]);
         for (u32 i = gwarp; i < nh; i += warps) {
             const u32 u = heavy[i];
@@ -370,19 +367,19 @@ __global__ void __launch_bounds__(PICK_BLOCK) k_match_loop(DGraph g, u32 *vcmap,
             const u32 h = pick_block<false, true>(g, vcmap, u, round_seed, sm);
             if (threadIdx.x == 0) hn[u] = h;
         }
-        grid.sync();
+        if (!grid_barrier(bar, err)) return;
         // still unmatched with a target: next round's list
         for (u64 i = gtid; i < cnt; i += gsize) {
             const u32 u = list[i];
             if (__ldcg(&vcmap[u]) == SENTINEL && __ldcg(&hn[u]) != SENTINEL) list2[atomicAdd(&ctr[0], 1u)] = u;
         }
-        grid.sync();
+        if (!grid_barrier(bar, err)) return;
         cnt = __ldcg(&ctr[0]);
         u32 *t = list;
         list = list2;
         list2 = t;
         if (gtid == 0) ctr[3] = round + 1;
-        grid.sync();  // every thread has read ctr[0] before the next round clears it
+        if (!grid_barrier(bar, err)) return;  // every thread has read ctr[0] before the next round clears it
     }
 }
 
@@ -529,19 +526,23 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
     if (n <= std::min<u32>(ctx.tune.match_coop_max_n, MATCH_COOP_MAX_N) && g.m <= ctx.tune.match_coop_max_m)
         HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_loop, PICK_BLOCK, 0));
     if (per_sm > 0) {
-        u32 *ctr = &ctx.d_status->cnt[8];  // 5 words, cleared below
-        HP_CUDA(cudaMemsetAsync(ctr, 0, 5 * sizeof(u32), ctx.stream));
+        u32 *ctr = &ctx.d_status->cnt[8];  // 5 words, then the barrier's 2 words; cleared below
+        u32 *bar = &ctx.d_status->cnt[13];
+        u32 *err = &ctx.d_status->err;
+        HP_CUDA(cudaMemsetAsync(ctr, 0, 7 * sizeof(u32), ctx.stream));
         const u32 want = (u32) std::max<u64>(1, ((u64) n + PICK_BLOCK - 1) / PICK_BLOCK);
         const u32 grid = std::min<u32>(want, (u32) (per_sm * ctx.sm_count));
         DGraph gg = g;
         u32 *pl = list, *pl2 = list2;
         u32 cnt0 = n;
         u32 sd = seed;
-        void *args[] = {&gg, &vcmap, &hn, &pl, &pl2, &cnt0, &claim, &heavy, &huge, &ctr, &sd};
+        void *args[] = {&gg, &vcmap, &hn, &pl, &pl2, &cnt0, &claim, &heavy, &huge, &ctr, &sd, &bar, &err};
         HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_match_loop, dim3(grid), dim3(PICK_BLOCK), args, 0,
                                             ctx.stream));
         note_launch();
-        if (ctx.read_status().cnt[12]) throw HpError{HP_ERR_DEVICE, "matching did not converge"};
+        const DevStatus &st = ctx.read_status();
+        if (st.err & DEV_ERR_SPIN) throw HpError{HP_ERR_DEVICE, "matching loop: a grid barrier wait gave up"};
+        if (st.cnt[12]) throw HpError{HP_ERR_DEVICE, "matching did not converge"};
     } else {
         u32 cnt = n;
         u32 round = 0, epoch = 0;

@@ -183,6 +183,10 @@ int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t
  * 0 = never), "jet_fused_max_n" / "jet_fused_max_m" (the whole refinement loop
  * of a level in one single-block launch up to these sizes, vertices capped at
  * 65536, when k <= 1024, or k <= 256 for the mapping objective; 0 = never),
+ * "jet_coop_max_n" / "jet_coop_max_m" / "jet_coop_max_deg" (likewise as one
+ * cooperative grid of 1024-thread blocks for larger sparse levels, up to this
+ * many vertices, entries and entries per vertex; 0 = never), "jet_coop_rows"
+ * (vertices per block of that grid),
  * "jet_hub_deg" (Jet connectivity passes with k <= 256: rows longer than this
  * are split into chunks of this many entries, one warp each; 64..4096).
  * Unknown names return HP_ERR_ARG. No counterpart in the reference. */

@@ -187,8 +187,17 @@ def test_rebalance_parity(ctx, gname, objective):
         dg.free()
 
 
+# Level-loop implementations of jet_refine: one block, a cooperative grid, or
+# one launch (graph) per step.
+LOOP_TUNES = {"block": {"jet_fused_max_n": 65536, "jet_fused_max_m": 1 << 30, "jet_coop_max_n": 0},
+              "grid": {"jet_fused_max_n": 0, "jet_coop_max_n": 65536, "jet_coop_max_m": 1 << 30,
+                       "jet_coop_max_deg": 1 << 20},
+              "kernels": {"jet_fused_max_n": 0, "jet_coop_max_n": 0}}
+
+
+@pytest.mark.parametrize("loop", sorted(LOOP_TUNES))
 @pytest.mark.parametrize("ultra", [False, True])
-def test_jet_refine_parity(ctx, ultra):
+def test_jet_refine_parity(ctx, ultra, loop):
     g = H.Graph.rmat(13, 8, seed=21)
     k = 32
     og = to_oracle(g)
@@ -196,15 +205,45 @@ def test_jet_refine_parity(ctx, ultra):
     lmax = O.lmax(g.total_weight(), k, 0.03)
     cut = O.edge_cut(og, part)
     maxw = int(np.bincount(part, minlength=k).max())
-    dg = ctx.upload(g)
+    c = H.Context(0, 1 << 30)
     try:
-        pg, cg, wg = ctx.jet_refine(dg, k, lmax, part, cut, maxw, ultra=ultra, level=1)
+        for name, v in LOOP_TUNES[loop].items():
+            c.tune(name, v)
+        dg = c.upload(g)
+        try:
+            pg, cg, wg = c.jet_refine(dg, k, lmax, part, cut, maxw, ultra=ultra, level=1)
+        finally:
+            dg.free()
     finally:
-        dg.free()
+        c.close()
     po, co, wo = O.jet_refine(og, k, lmax, ultra, 1, part, cut, maxw)
     assert (cg, wg) == (co, wo)
     np.testing.assert_array_equal(pg, po)
     assert cg == O.edge_cut(og, pg)
+
+
+@pytest.mark.parametrize("loop", sorted(LOOP_TUNES))
+def test_level_loops_pipelines(ctx, loop):
+    # whole pipelines (cut and J objectives, default and ultra) with every
+    # level of at most 65536 vertices on one level-loop implementation
+    cases = [(H.Graph.grid(200, 150), 16, "default"), (H.Graph.rmat(15, 8, seed=5), 64, "ultra")]
+    m = H.Graph.rgg3d(40000, 14.0, 1, 100, seed=8, explicit_vw=True)
+    c = H.Context(0, 2 << 30)
+    try:
+        for name, v in LOOP_TUNES[loop].items():
+            c.tune(name, v)
+        for g, k, config in cases:
+            part, cut = c.partition(g, k, 0.03, config, 7)
+            opart, ocut = O.partition(to_oracle(g), k, 0.03, config == "ultra", 7)
+            assert cut == ocut
+            np.testing.assert_array_equal(part, opart)
+        for mode in ("IM", "HM"):
+            mp, J = c.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, mode, 3)
+            want_m, want_j = ctx.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, mode, 3)
+            assert J == want_j
+            np.testing.assert_array_equal(mp, want_m)
+    finally:
+        c.close()
 
 
 @pytest.mark.parametrize("name,g,k", [("grid256_k16", H.Graph.grid(256, 256), 16),
@@ -280,7 +319,8 @@ def test_direct_launch_paths_equal(ctx):
     want_m, want_j = ctx.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, "HM", 3)
     c2 = H.Context(0, 2 << 30)
     try:
-        for name in ("jet_graph_max_m", "order_small_n", "match_coop_max_n", "match_coop_max_m", "jet_fused_max_n"):
+        for name in ("jet_graph_max_m", "order_small_n", "match_coop_max_n", "match_coop_max_m", "jet_fused_max_n",
+                     "jet_coop_max_n"):
             c2.tune(name, 0)
         c2.tune("jet_hub_deg", 4096)
         part, cut = c2.partition(g, 64, 0.03, "default", 7)
