@@ -7,6 +7,9 @@
 #pragma once
 #include <cstdint>
 #include <cstddef>
+#include <memory>
+#include <type_traits>
+#include <utility>
 #include <vector>
 #include <string>
 
@@ -30,16 +33,41 @@ constexpr u32 NO_MOVE = 0xFFFFFFFFu - 3u;
 constexpr u32 NO_BLOCK_ID = 0xFFFFFFFFu;
 constexpr u32 SENTINEL = 0xFFFFFFFFu;
 
+// Allocator whose resize() leaves elements of trivially constructible types
+// uninitialised, so that large host arrays are first touched (and their pages
+// faulted in) by the threads that fill them rather than by one zero-fill.
+// Every resize() of such a vector is followed by writes to all new elements.
+template<typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template<typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template<typename U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template<typename U>
+    void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new ((void *) p) U;
+    }
+    template<typename U, typename... Args>
+    void construct(U *p, Args &&...args) {
+        ::new ((void *) p) U(std::forward<Args>(args)...);
+    }
+};
+template<typename T>
+using hvec = std::vector<T, NoInitAlloc<T> >;
+
 // A host CSR graph. `m` counts directed entries (2x the undirected edges), as
 // the reference stores it (src/datastructures/host_graph.h:195). Empty `ew` /
 // `vw` mean unit weights ("uniform" in the reference).
 struct HostCSR {
     u32 n = 0;
     u32 m = 0;
-    std::vector<u32> xadj;  // n+1
-    std::vector<u32> adj;   // m
-    std::vector<s32> ew;    // m or empty
-    std::vector<s32> vw;    // n or empty
+    hvec<u32> xadj;  // n+1
+    hvec<u32> adj;   // m
+    hvec<s32> ew;    // m or empty
+    hvec<s32> vw;    // n or empty
     s64 total_vw() const {
         if (vw.empty()) return (s64) n;
         s64 s = 0;

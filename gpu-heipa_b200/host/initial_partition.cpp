@@ -19,10 +19,12 @@ struct IGraph {
 IGraph to_igraph(const HostCSR &g) {
     IGraph r;
     r.n = g.n;
-    r.xadj = g.xadj;
-    r.adj = g.adj;
-    r.ew = g.ew.empty() ? std::vector<s32>(g.m, 1) : g.ew;
-    r.vw = g.vw.empty() ? std::vector<s32>(g.n, 1) : g.vw;
+    r.xadj.assign(g.xadj.begin(), g.xadj.end());
+    r.adj.assign(g.adj.begin(), g.adj.end());
+    if (g.ew.empty()) r.ew.assign(g.m, 1);
+    else r.ew.assign(g.ew.begin(), g.ew.end());
+    if (g.vw.empty()) r.vw.assign(g.n, 1);
+    else r.vw.assign(g.vw.begin(), g.vw.end());
     r.W = 0;
     for (s32 w: r.vw) r.W += w;
     if (r.xadj.empty()) r.xadj.assign(1, 0);

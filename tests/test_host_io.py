@@ -111,6 +111,47 @@ def test_metis_reader_errors(tmp_path, text):
         H.Graph.read_metis(p)
 
 
+def test_metis_reader_large_files(tmp_path):
+    # Bodies above 4 MB are parsed in chunks on all host threads; the result
+    # and the error behaviour must be those of the line-by-line reader.
+    g = H.Graph.rmat(16, 16, seed=2)
+    vw = (np.arange(g.n) % 7 + 1).astype(np.int32)
+    g = H.Graph(g.xadj, g.adj, g.ew, vw)
+    path = tmp_path / "big.metis"
+    g.write_metis(path)
+    assert os.path.getsize(path) > (8 << 20)
+    lines = open(path).read().split("\n")
+    # comment lines inside the body and ignored lines after the last vertex
+    body = lines[1:1 + g.n]
+    mid = len(body) // 2
+    text = "\n".join([lines[0]] + body[:mid] + ["% a comment", "%"] + body[mid:] + ["trailing text 1 2 3", ""])
+    path.write_text(text)
+    r = H.Graph.read_metis(path)
+    np.testing.assert_array_equal(r.xadj, g.xadj)
+    np.testing.assert_array_equal(r.adj, g.adj)
+    np.testing.assert_array_equal(r.ew, g.ew)
+    np.testing.assert_array_equal(r.vw, vw)
+    # errors deep inside a large body
+    bad_id = list(body)
+    bad_id[mid] = f"{vw[mid]} {g.n + 1} 3"
+    bad_weight = list(body)
+    bad_weight[mid + 5] = bad_weight[mid + 5].rsplit(" ", 1)[0]
+    bad_char = list(body)
+    bad_char[mid + 9] = bad_char[mid + 9] + " x"
+    for b in (bad_id, bad_weight, bad_char, body[:-3]):
+        path.write_text("\n".join([lines[0]] + b) + "\n")
+        with pytest.raises(H.HeiPaError):
+            H.Graph.read_metis(path)
+
+
+def test_metis_writer_large_partition(tmp_path):
+    part = (np.arange(700000, dtype=np.uint64) * 2654435761 % 512).astype(np.uint32)
+    path = tmp_path / "part.txt"
+    H.write_partition(path, part)
+    got = np.loadtxt(path, dtype=np.uint32)
+    np.testing.assert_array_equal(got, part)
+
+
 def test_metis_reader_missing_file(tmp_path):
     with pytest.raises(H.HeiPaError):
         H.Graph.read_metis(tmp_path / "missing.metis")
