@@ -135,110 +135,189 @@ void graph_download(Ctx &ctx, const DGraph &g, u32 *xadj, u32 *adj, s32 *ew, s32
     ctx.sync();
 }
 
-// ---- induced subgraph (hierarchical multisection) ------------------------------
+// ---- induced subgraphs (hierarchical multisection): all parts in one pass --------------
 
-// Per-vertex count of neighbours inside the block (one warp per vertex).
-__global__ void k_sub_degrees(DGraph g, const u32 *part, u32 id, u32 *deg) {
+struct IndPart {
+    u32 *rowptr, *rowlen, *adj;
+    s32 *ew, *vw;
+    u32 *n_to_o;
+    u32 n, vstart;
+    u64 m, ebase;
+};
+
+constexpr u32 IND_SMEM_K = 1024;  // per-block part histograms in shared memory up to this k
+
+// Same-part degree of every vertex, and per part: vertices, entries, vertex
+// weight (block histograms in shared memory for small k).
+__global__ void k_ind_count(DGraph g, const u32 *part, u32 k, u32 *deg, u32 *cnt_v, unsigned long long *cnt_e,
+                            unsigned long long *sum_vw, u32 *err) {
+    __shared__ u32 sv[IND_SMEM_K];
+    __shared__ unsigned long long se[IND_SMEM_K], sw[IND_SMEM_K];
+    const bool local = k <= IND_SMEM_K;
+    if (local) {
+        for (u32 p = threadIdx.x; p < k; p += blockDim.x) {
+            sv[p] = 0;
+            se[p] = 0;
+            sw[p] = 0;
+        }
+        __syncthreads();
+    }
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     for (u32 u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < g.n; u += warps) {
-        u32 c = 0;
-        if (part[u] == id) {
-            const u64 beg = g.rowptr[u];
-            const u32 len = g.rowlen[u];
-            for (u32 t = lane_id(); t < len; t += 32) c += part[g.adj[beg + t]] == id;
-            c = warp_sum<u32>(c);
+        const u32 p = part[u];
+        if (p >= k) {
+            if (lane_id() == 0) {
+                set_error(err, DEV_ERR_RANGE);
+                deg[u] = 0;
+            }
+            continue;
         }
-        if (lane_id() == 0) deg[u] = c;
+        const u64 beg = g.rowptr[u];
+        const u32 len = g.rowlen[u];
+        u32 c = 0;
+        for (u32 t = lane_id(); t < len; t += 32) c += part[g.adj[beg + t]] == p;
+        c = warp_sum<u32>(c);
+        if (lane_id() == 0) {
+            deg[u] = c;
+            const s32 w = g_vw(g, u);
+            if (local) {
+                atomicAdd(&sv[p], 1u);
+                atomicAdd(&se[p], (unsigned long long) c);
+                atomicAdd(&sw[p], (unsigned long long) (long long) w);
+            } else {
+                atomicAdd(&cnt_v[p], 1u);
+                atomicAdd(&cnt_e[p], (unsigned long long) c);
+                atomicAdd(&sum_vw[p], (unsigned long long) (long long) w);
+            }
+        }
+    }
+    if (local) {
+        __syncthreads();
+        for (u32 p = threadIdx.x; p < k; p += blockDim.x)
+            if (sv[p]) {
+                atomicAdd(&cnt_v[p], sv[p]);
+                atomicAdd(&cnt_e[p], se[p]);
+                atomicAdd(&sum_vw[p], sw[p]);
+            }
     }
 }
 
-// Writes the rows of the block's vertices; row order is kept with a warp
-// ballot compaction.
-__global__ void k_sub_fill(DGraph g, const u32 *part, u32 id, const u32 *local, const u32 *eoff, DGraph s) {
+// Local ids (rank within the part in ascending vertex id, from the sorted
+// order), composed root ids, row offsets, row lengths and vertex weights.
+__global__ void k_ind_local(DGraph g, const u32 *skey, const u32 *sval, const u32 *pre, const u32 *deg,
+                            const IndPart *T, const u32 *n_to_o_parent, u32 *local_of) {
+    for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < g.n; i += gridDim.x * blockDim.x) {
+        const u32 p = skey[i], u = sval[i];
+        const IndPart P = T[p];
+        const u32 lu = i - P.vstart;
+        local_of[u] = lu;
+        P.n_to_o[lu] = n_to_o_parent[u];
+        P.rowptr[lu] = (u32) (pre[i] - P.ebase);
+        P.rowlen[lu] = deg[u];
+        P.vw[lu] = g_vw(g, u);
+        if (lu + 1 == P.n) P.rowptr[P.n] = (u32) P.m;
+    }
+}
+
+// Rows of every subgraph, in parent row order (warp ballot compaction).
+__global__ void k_ind_fill(DGraph g, const u32 *part, const u32 *local_of, const IndPart *T, u32 k) {
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     for (u32 u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < g.n; u += warps) {
-        if (part[u] != id) continue;
-        const u32 lu = local[u];
+        const u32 p = part[u];
+        if (p >= k) continue;
+        const IndPart P = T[p];
         const u64 beg = g.rowptr[u];
         const u32 len = g.rowlen[u];
-        u64 out = eoff[u];
-        if (lane_id() == 0) {
-            s.rowptr[lu] = (u32) out;
-            s.vw[lu] = g_vw(g, u);
-        }
+        u64 out = P.rowptr[local_of[u]];
         for (u32 t0 = 0; t0 < len; t0 += 32) {
-            u32 t = t0 + lane_id();
+            const u32 t = t0 + lane_id();
             bool keep = false;
             u32 v = 0;
             if (t < len) {
                 v = g.adj[beg + t];
-                keep = part[v] == id;
+                keep = part[v] == p;
             }
-            unsigned mask = __ballot_sync(FULL, keep);
+            const unsigned mask = __ballot_sync(FULL, keep);
             if (keep) {
-                u64 pos = out + __popc(mask & ((1u << lane_id()) - 1u));
-                s.adj[pos] = local[v];
-                s.ew[pos] = g_ew(g, beg + t);
+                const u64 pos = out + __popc(mask & ((1u << lane_id()) - 1u));
+                P.adj[pos] = local_of[v];
+                P.ew[pos] = g_ew(g, beg + t);
             }
             out += __popc(mask);
         }
     }
 }
 
-__global__ void k_sub_rowlen(DGraph s, u32 m) {
-    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < s.n; u += gridDim.x * blockDim.x) {
-        u32 end = (u + 1 < s.n) ? s.rowptr[u + 1] : m;
-        s.rowlen[u] = end - s.rowptr[u];
-        if (u + 1 == s.n) s.rowptr[s.n] = m;
+void graph_induced_all(Ctx &ctx, const DGraph &g, const u32 *part, u32 k, const u32 *n_to_o_parent,
+                       std::vector<DGraph> &subs, std::vector<u32 *> &n_to_o) {
+    subs.assign(k, DGraph{});
+    n_to_o.assign(k, nullptr);
+    if (g.n == 0 || k == 0) return;
+    // per-part sizes (front allocations below must not sit under scratch:
+    // the scratch of this function is taken from the back)
+    ScratchScope ss(ctx.arena);
+    u32 *deg = ctx.balloc<u32>(g.n);
+    u32 *cnt_v = ctx.balloc<u32>(k);
+    unsigned long long *cnt_e = ctx.balloc<unsigned long long>(k);
+    unsigned long long *sum_vw = ctx.balloc<unsigned long long>(k);
+    HP_CUDA(cudaMemsetAsync(cnt_v, 0, sizeof(u32) * k, ctx.stream));
+    HP_CUDA(cudaMemsetAsync(cnt_e, 0, sizeof(unsigned long long) * k, ctx.stream));
+    HP_CUDA(cudaMemsetAsync(sum_vw, 0, sizeof(unsigned long long) * k, ctx.stream));
+    ctx.zero_status();
+    k_ind_count<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, k, deg, cnt_v, cnt_e, sum_vw,
+                                                                          &ctx.d_status->err); note_launch();
+    HP_LAUNCH_CHECK();
+    std::vector<u32> hv(k);
+    std::vector<unsigned long long> he(k), hw(k);
+    HP_CUDA(cudaMemcpyAsync(hv.data(), cnt_v, sizeof(u32) * k, cudaMemcpyDeviceToHost, ctx.stream));
+    HP_CUDA(cudaMemcpyAsync(he.data(), cnt_e, sizeof(unsigned long long) * k, cudaMemcpyDeviceToHost, ctx.stream));
+    HP_CUDA(cudaMemcpyAsync(hw.data(), sum_vw, sizeof(unsigned long long) * k, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.check_device_error();
+    // per-part arrays (front of the arena, part after part)
+    std::vector<IndPart> T(k);
+    u64 vstart = 0, ebase = 0;
+    for (u32 p = 0; p < k; ++p) {
+        IndPart &P = T[p];
+        P.n = hv[p];
+        P.m = he[p];
+        P.vstart = (u32) vstart;
+        P.ebase = ebase;
+        vstart += P.n;
+        ebase += P.m;
+        if (P.n == 0) continue;
+        DGraph &s = subs[p];
+        s.n = P.n;
+        s.m = s.cap = P.m;
+        s.rowptr = P.rowptr = ctx.falloc<u32>((u64) P.n + 1);
+        s.rowlen = P.rowlen = ctx.falloc<u32>(P.n);
+        s.adj = P.adj = ctx.falloc<u32>(P.m);
+        s.ew = P.ew = ctx.falloc<s32>(P.m);
+        s.vw = P.vw = ctx.falloc<s32>(P.n);
+        s.total_vw = (s64) hw[p];
+        n_to_o[p] = P.n_to_o = ctx.falloc<u32>(P.n);
     }
+    if (ebase > 0xFFFFFFFFull) throw HpError{HP_ERR_ARG, "induced subgraphs exceed 32-bit offsets"};
+    IndPart *dT = ctx.balloc<IndPart>(k);
+    HP_CUDA(cudaMemcpyAsync(dT, T.data(), sizeof(IndPart) * k, cudaMemcpyHostToDevice, ctx.stream));
+    // vertices grouped by part, ascending id within each part (stable sort)
+    u32 *skey = ctx.balloc<u32>(g.n);
+    u32 *sval = ctx.balloc<u32>(g.n);
+    HP_CUDA(cudaMemcpyAsync(skey, part, sizeof(u32) * g.n, cudaMemcpyDeviceToDevice, ctx.stream));
+    device_iota(ctx, sval, g.n);
+    radix_sort_pairs<u32>(ctx, skey, sval, g.n, 0, bits_for(k));
+    // entry offsets in that order: parts are contiguous, so part p's rows
+    // start at its ebase
+    u32 *pre = ctx.balloc<u32>(g.n);
+    device_scan<u32>(
+        ctx, g.n, [=] __device__(u64 i) -> u32 { return deg[sval[i]]; },
+        [=] __device__(u64 i, u32 q, u32) { pre[i] = q; }, (u32 *) nullptr);
+    u32 *local_of = ctx.balloc<u32>(g.n);
+    k_ind_local<<<ctx.grid(g.n, BLOCK), BLOCK, 0, ctx.stream>>>(g, skey, sval, pre, deg, dT, n_to_o_parent,
+                                                                local_of); note_launch();
+    k_ind_fill<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, local_of, dT, k); note_launch();
+    HP_LAUNCH_CHECK();
+    ctx.sync();  // the scratch (table, order, local ids) is released on return
 }
 
-DGraph graph_induced(Ctx &ctx, const DGraph &g, const u32 *part, u32 id, u32 *n_to_o_out, u32 &sub_n) {
-    ScratchScope ss(ctx.arena);
-    u32 *counts = &ctx.d_status->cnt[0];
-    ctx.zero_counters();
-    u32 *local = ctx.balloc<u32>(g.n);
-    u32 *eoff = ctx.balloc<u32>((u64) g.n + 1);
-    u32 *deg = ctx.balloc<u32>(g.n);
-    device_scan<u32>(
-        ctx, g.n, [=] __device__(u64 i) -> u32 { return part[i] == id ? 1u : 0u; },
-        [=] __device__(u64 i, u32 p, u32 v) {
-            if (v) {
-                local[i] = p;
-                n_to_o_out[p] = (u32) i;
-            }
-        },
-        counts + 0);
-    k_sub_degrees<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, id, deg); note_launch();
-    HP_LAUNCH_CHECK();
-    device_scan<u32>(
-        ctx, g.n, [=] __device__(u64 i) -> u32 { return deg[i]; }, [=] __device__(u64 i, u32 p, u32) { eoff[i] = p; },
-        counts + 1);
-    const DevStatus &st = ctx.read_status();
-    sub_n = st.cnt[0];
-    const u32 sub_m = st.cnt[1];
-    DGraph s;
-    s.n = sub_n;
-    s.cap = sub_m;
-    s.m = sub_m;
-    s.rowptr = ctx.falloc<u32>((u64) sub_n + 1);
-    s.rowlen = ctx.falloc<u32>(sub_n);
-    s.adj = ctx.falloc<u32>(sub_m);
-    s.ew = ctx.falloc<s32>(sub_m);
-    s.vw = ctx.falloc<s32>(sub_n);
-    if (sub_n == 0) return s;
-    k_sub_fill<<<ctx.grid((u64) g.n * 32, BLOCK), BLOCK, 0, ctx.stream>>>(g, part, id, local, eoff, s); note_launch();
-    k_sub_rowlen<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(s, sub_m); note_launch();
-    HP_LAUNCH_CHECK();
-    // total vertex weight of the subgraph
-    ctx.zero_counters();
-    const s32 *svw = s.vw;
-    long long *sum = &ctx.d_status->sum[0];
-    device_scan<long long>(
-        ctx, sub_n, [=] __device__(u64 i) -> long long { return svw[i]; }, [=] __device__(u64, long long, long long) {},
-        sum);
-    s.total_vw = ctx.read_status().sum[0];
-    return s;
-}
 
 } // namespace hp

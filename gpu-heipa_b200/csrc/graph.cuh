@@ -40,8 +40,14 @@ DGraph graph_from_device(Ctx &ctx, u32 n, u64 m, const u32 *d_xadj, const u32 *d
 // Writes a compact CSR copy of g to host arrays (xadj n+1, adj m, ew m, vw n).
 void graph_download(Ctx &ctx, const DGraph &g, u32 *xadj, u32 *adj, s32 *ew, s32 *vw);
 
-// Induced subgraph of the vertices with part[u] == id (vertex order and row
-// order kept); n_to_o receives parent ids. hierarchical_multisection.h:104-206.
-DGraph graph_induced(Ctx &ctx, const DGraph &g, const u32 *part, u32 id, u32 *n_to_o_out, u32 &sub_n);
+// All subgraphs induced by parts 0..k-1 of `part`, in one pass over g
+// (hierarchical_multisection.h:104-206 induces them one part at a time):
+// subs[p] holds the vertices with part p in ascending id and, for each, its
+// same-part neighbours in row order, renumbered to local ids (an empty graph
+// when part p is empty); n_to_o[p] maps its vertices through n_to_o_parent
+// (parent id -> root id). Arrays are allocated from the front of the arena,
+// part after part.
+void graph_induced_all(Ctx &ctx, const DGraph &g, const u32 *part, u32 k, const u32 *n_to_o_parent,
+                       std::vector<DGraph> &subs, std::vector<u32 *> &n_to_o);
 
 } // namespace hp

@@ -29,10 +29,6 @@ __global__ void k_scatter_leaf(const u32 *tmp, const u32 *n_to_o, u32 n, u32 off
         global_part[n_to_o[u]] = offset + tmp[u];
 }
 
-__global__ void k_compose(const u32 *outer, const u32 *inner, u32 n, u32 *out) {
-    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) out[u] = outer[inner[u]];
-}
-
 // Downloads the coarsest graph with rows in canonical (sorted) order.
 HostCSR download_sorted(Ctx &ctx, const DGraph &g) {
     HostCSR h;
@@ -287,21 +283,15 @@ void hm_solve(Ctx &ctx, const DGraph &g, const std::vector<u32> &hier, double ep
         if (leaf) break;
         std::vector<HmTask> next;
         for (HmTask &t: cur) {
+            // the k_here subgraphs of this task in one pass over its graph
+            std::vector<DGraph> subs;
+            std::vector<u32 *> sub_n_to_o;
+            graph_induced_all(ctx, t.g, t.part, k_here, t.n_to_o, subs, sub_n_to_o);
             for (u32 id = 0; id < k_here; ++id) {
-                const size_t m2 = ctx.arena.front_mark();
-                u32 *local = ctx.falloc<u32>(t.g.n);
-                u32 sub_n = 0;
-                DGraph sg = graph_induced(ctx, t.g, t.part, id, local, sub_n);
-                if (sub_n == 0) {
-                    ctx.arena.front_release(m2);
-                    continue;
-                }
-                u32 *sub_n_to_o = ctx.falloc<u32>(sub_n);
-                k_compose<<<ctx.grid(sub_n, BLOCK), BLOCK, 0, ctx.stream>>>(t.n_to_o, local, sub_n, sub_n_to_o); note_launch();
-                HP_LAUNCH_CHECK();
+                if (subs[id].n == 0) continue;
                 HmTask c;
-                c.g = sg;
-                c.n_to_o = sub_n_to_o;
+                c.g = subs[id];
+                c.n_to_o = sub_n_to_o[id];
                 c.identifier = t.identifier;
                 c.identifier.push_back(id);
                 next.push_back(std::move(c));
