@@ -60,6 +60,7 @@ _SIG = {
     "hp_edge_cut": (_int, [_vp, _vp, _vp, _vp]),
     "hp_comm_cost": (_int, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
     "hp_edge_cut_noalloc": (_int, [_u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "hp_selftest_barrier_timeout": (_int, [ctypes.c_int, _u32, _vp, _vp]),
     "hp_partition": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_partition_graph": (_int, [_vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_map": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
@@ -255,6 +256,20 @@ class Server:
 def kernel_launches():
     """Kernels launched by this process through the library so far."""
     return int(_L.hp_kernel_launches())
+
+
+DEVERR_SPIN = 8  # device error bit: a bounded wait gave up
+
+
+def selftest_barrier_timeout(device=0, blocks=4):
+    """Runs hp_selftest_barrier_timeout: a cooperative kernel in which one
+    block never reaches the grid barrier. Returns (error bits, kernel ms)."""
+    err = ctypes.c_uint32(0)
+    ms = ctypes.c_double(0.0)
+    rc = _L.hp_selftest_barrier_timeout(device, blocks, ctypes.byref(err), ctypes.byref(ms))
+    if rc != 0:
+        raise HeiPaError(rc, "barrier self-test failed")
+    return err.value, ms.value
 
 
 def edge_cut_noalloc(n, m, d_xadj, d_adj, d_ew, part, stream=0):

@@ -174,6 +174,17 @@ int hp_last_solve_maxw(const hp_ctx *ctx, int32_t *initial_maxw, int32_t *final_
  * per-level "n m" lines of solver.h:358; HP_ERR_ARG past the last level. */
 int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t *m);
 
+/* Diagnostics of the bounded waits: launches `blocks` (>= 2, all resident at
+ * once) cooperative blocks of which one never reaches a grid barrier; the
+ * others give up after the barrier's bounded wait (about a second), set
+ * HP_DEVERR_SPIN in the kernel's error word and end. *err_bits receives that
+ * word, *ms (if non-NULL) the kernel's duration. Returns HP_OK when the call
+ * ran (whatever the bits), HP_ERR_ARG for a bad device or block count. The
+ * cooperative Jet level loop and matching loop use the same barrier. No
+ * counterpart in the reference. */
+#define HP_DEVERR_SPIN 8u
+int hp_selftest_barrier_timeout(int device, uint32_t blocks, uint32_t *err_bits, double *ms);
+
 /* Sets a size threshold that chooses between equivalent implementations
  * (results are identical; only the launch structure changes): "jet_graph_max_m"
  * (levels up to this many CSR entries replay Jet iterations as CUDA graphs;
