@@ -225,14 +225,15 @@ def barrier(world):
 
 
 def cpu_oracle_run(H, wl, args):
-    """Times the oracle on the workload's bounded sample: (edges, seconds, objective)."""
+    """Times the oracle on the workload's bounded sample on all host threads:
+    (edges, seconds, objective, threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     g = make_graph(H, wl["sample"], args.seed)
     og = O.Graph(g.xadj, g.adj, g.ew, g.vw)
     t0 = time.perf_counter()
     obj = oracle_solve(O, og, wl, args)
-    return g.m // 2, time.perf_counter() - t0, obj
+    return g.m // 2, time.perf_counter() - t0, obj, O.threads()
 
 
 def run_reference(args, world, rank):
@@ -240,9 +241,9 @@ def run_reference(args, world, rank):
         return 0
     import gpu_heipa as H
     wl = WORKLOADS[args.workload]
-    times, edges = [], 0
+    times, edges, cores = [], 0, 1
     for i in range(args.warmup + args.steps):
-        e, dt, _ = cpu_oracle_run(H, wl, args)
+        e, dt, _, cores = cpu_oracle_run(H, wl, args)
         if i >= args.warmup:
             times.append(dt)
             edges = e
@@ -254,7 +255,7 @@ def run_reference(args, world, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
         "config": {"workload": wl["desc"], "config": config_of(wl, args), "parallelism": "cpu"},
         "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 1, "kind": "port", "sample": sample_desc(wl)},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": cores, "kind": "port", "sample": sample_desc(wl)},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -510,8 +511,8 @@ def run_ours(args, world, rank, local):
                                   if timing[x]["ms"] else None} for x in timing}}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        e, dt, cobj = cpu_oracle_run(H, wl, args)
-        cpu = {"value": e / dt, "unit": "edges/s", "cores": 1, "kind": "port",
+        e, dt, cobj, cores = cpu_oracle_run(H, wl, args)
+        cpu = {"value": e / dt, "unit": "edges/s", "cores": cores, "kind": "port",
                "sample": f"one solve of {sample_desc(wl)}, {dt:.1f} s", "objective": cobj}
     line = {
         "metric": "partition_throughput", "value": value, "unit": "edges/s", "n_gpus": world,

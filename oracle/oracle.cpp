@@ -29,6 +29,8 @@
 #include <numeric>
 #include <vector>
 
+#include <omp.h>
+
 #include "../gpu-heipa_b200/host/hp_types.h"
 #include "../gpu-heipa_b200/host/initial_partition.h"
 
@@ -194,7 +196,9 @@ u32 match(const HostCSR &g, std::vector<u32> &mapping) {
     const u32 seed = MATCH_SEED;
     const bool uniform = g.ew.empty();
     // initial pick: two_hop_matching.h:276-304
-    for (u32 i = 0; i < n; ++i) {
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (s64 ii = 0; ii < (s64) n; ++ii) {  // reads vcmap, writes hn[i] only
+        const u32 i = (u32) ii;
         if (uniform) {
             u32 d = deg(g, i);
             if (d == 0) continue;
@@ -235,7 +239,9 @@ u32 match(const HostCSR &g, std::vector<u32> &mapping) {
             for (u32 u: list)  // commit_p3
                 if (vcmap[u] == SENTINEL - 1) vcmap[u] = SENTINEL;
         }
-        for (u32 u: list) {  // re-pick
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (s64 li = 0; li < (s64) list.size(); ++li) {  // re-pick (reads vcmap, writes hn[u] only)
+            const u32 u = list[(size_t) li];
             if (vcmap[u] != SENTINEL || hn[u] == SENTINEL || vcmap[hn[u]] == SENTINEL) continue;
             hn[u] = pick(g, vcmap, u, round_seed, false);
         }
@@ -327,34 +333,56 @@ HostCSR contract(const HostCSR &g, const std::vector<u32> &mapping, u32 nc) {
         std::vector<u32> cur(moff.begin(), moff.end() - 1);
         for (u32 u = 0; u < g.n; ++u) mem[cur[mapping[u]]++] = u;
     }
+    // coarse rows on all threads, each with its own accumulator: pass 0
+    // counts the distinct neighbours of every coarse vertex, pass 1 writes the
+    // sorted rows at their offsets
     c.xadj.assign(nc + 1, 0);
-    std::vector<s32> acc(nc, 0);
-    std::vector<u8> seen(nc, 0);
-    std::vector<u32> touched;
-    for (u32 cu = 0; cu < nc; ++cu) {
-        touched.clear();
-        for (u32 t = moff[cu]; t < moff[cu + 1]; ++t) {
-            u32 u = mem[t];
-            for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
-                u32 cv = mapping[g.adj[j]];
-                if (cv == cu) continue;
-                if (!seen[cv]) {
-                    seen[cv] = 1;
-                    touched.push_back(cv);
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            for (u32 i = 0; i < nc; ++i) c.xadj[i + 1] += c.xadj[i];
+            c.m = c.xadj[nc];
+            c.adj.resize(c.m);
+            c.ew.resize(c.m);
+        }
+#pragma omp parallel
+        {
+            std::vector<s32> acc(nc, 0);
+            std::vector<u8> seen(nc, 0);
+            std::vector<u32> touched;
+#pragma omp for schedule(dynamic, 256)
+            for (s64 ci = 0; ci < (s64) nc; ++ci) {
+                const u32 cu = (u32) ci;
+                touched.clear();
+                for (u32 t = moff[cu]; t < moff[cu + 1]; ++t) {
+                    u32 u = mem[t];
+                    for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
+                        u32 cv = mapping[g.adj[j]];
+                        if (cv == cu) continue;
+                        if (!seen[cv]) {
+                            seen[cv] = 1;
+                            touched.push_back(cv);
+                        }
+                        acc[cv] = wadd(acc[cv], EW(g, j));
+                    }
                 }
-                acc[cv] = wadd(acc[cv], EW(g, j));
+                if (pass == 0) {
+                    c.xadj[cu + 1] = (u32) touched.size();
+                } else {
+                    std::sort(touched.begin(), touched.end());
+                    u32 o = c.xadj[cu];
+                    for (u32 cv: touched) {
+                        c.adj[o] = cv;
+                        c.ew[o] = acc[cv];
+                        ++o;
+                    }
+                }
+                for (u32 cv: touched) {
+                    acc[cv] = 0;
+                    seen[cv] = 0;
+                }
             }
         }
-        std::sort(touched.begin(), touched.end());
-        for (u32 cv: touched) {
-            c.adj.push_back(cv);
-            c.ew.push_back(acc[cv]);
-            acc[cv] = 0;
-            seen[cv] = 0;
-        }
-        c.xadj[cu + 1] = (u32) c.adj.size();
     }
-    c.m = (u32) c.adj.size();
     return c;
 }
 
@@ -403,6 +431,26 @@ s32 lmax_of(s64 W, u32 k, double eps) { return (s32) std::ceil((1.0 + eps) * ((d
 // Jet refinement: jet_label_propagation.h and promap_jet_label_propagation.h
 // ---------------------------------------------------------------------------
 
+// Connectivity row of one vertex (rule R7: the blocks adjacent to u with
+// their connection weight, ascending id). One per thread: the per-vertex
+// loops of the Jet steps below read only state that the loop does not write,
+// so they run on all host threads with the same results as one thread.
+struct Conn {
+    std::vector<s32> acc;
+    std::vector<u32> touched;
+    void build(const HostCSR &g, const std::vector<u32> &map, u32 u) {
+        for (u32 b: touched) acc[b] = 0;
+        touched.clear();
+        for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
+            u32 b = map[g.adj[j]];
+            if (acc[b] == 0) touched.push_back(b);
+            acc[b] = wadd(acc[b], EW(g, j));
+        }
+        std::sort(touched.begin(), touched.end());
+    }
+    s32 of(u32 b) const { return acc[b]; }
+};
+
 struct Jet {
     const HostCSR *g = nullptr;
     u32 n = 0, k = 0;
@@ -412,24 +460,14 @@ struct Jet {
     std::vector<s32> D;  // k*k when promap
     std::vector<u32> map, dest_cache, dest_part, lock;
     std::vector<s32> bw, gain_cache, gain1;
-    // scratch for connectivity rows
-    std::vector<s32> acc;
-    std::vector<u32> touched;
+    std::vector<Conn> conns;  // one per host thread
 
     s32 dist(u32 a, u32 b) const { return D[(size_t) a * k + b]; }
-
-    // R7: the blocks adjacent to u with their connection weight, ascending id.
-    void conn(u32 u) {
-        for (u32 b: touched) acc[b] = 0;
-        touched.clear();
-        for (u32 j = g->xadj[u]; j < g->xadj[u + 1]; ++j) {
-            u32 b = map[g->adj[j]];
-            if (acc[b] == 0) touched.push_back(b);
-            acc[b] = wadd(acc[b], EW(*g, j));
-        }
-        std::sort(touched.begin(), touched.end());
+    Conn &conn(u32 u) {
+        Conn &c = conns[(size_t) omp_get_thread_num()];
+        c.build(*g, map, u);
+        return c;
     }
-    s32 conn_of(u32 b) const { return acc[b]; }
 };
 
 void jet_init(Jet &J, const HostCSR &g, u32 k, s32 lmax, const u32 *part) {
@@ -447,8 +485,8 @@ void jet_init(Jet &J, const HostCSR &g, u32 k, s32 lmax, const u32 *part) {
     J.dest_part.assign(g.n, NO_MOVE);
     J.lock.assign(g.n, 0);
     J.gain1.assign(g.n, 0);
-    J.acc.assign(k, 0);
-    J.touched.clear();
+    J.conns.assign((size_t) omp_get_max_threads(), Conn{});
+    for (Conn &c: J.conns) c.acc.assign(k, 0);
 }
 
 // jet_lp jet_label_propagation.h:182-354 (edge cut) and ProMap_jet_lp
@@ -456,21 +494,23 @@ void jet_init(Jet &J, const HostCSR &g, u32 k, s32 lmax, const u32 *part) {
 std::vector<u32> jet_lp(Jet &J, u32 ratio_pct) {
     const HostCSR &g = *J.g;
     const u32 n = J.n;
-    for (u32 u = 0; u < n; ++u) {  // best_block
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (s64 ui = 0; ui < (s64) n; ++ui) {  // best_block
+        const u32 u = (u32) ui;
         if (J.dest_cache[u] != NULL_PART) {
             J.dest_part[u] = J.dest_cache[u];
             continue;
         }
-        J.conn(u);
+        const Conn &C = J.conn(u);
         const u32 o = J.map[u];
         u32 best = NO_MOVE;
         s32 gain = 0;
         if (!J.promap) {
-            const s32 own = J.conn_of(o);
+            const s32 own = C.of(o);
             s32 bc = 0;
-            for (u32 b: J.touched) {
+            for (u32 b: C.touched) {
                 if (b == o) continue;
-                s32 c = J.conn_of(b);
+                s32 c = C.of(b);
                 if (c > bc) {
                     bc = c;
                     best = b;
@@ -482,10 +522,10 @@ std::vector<u32> jet_lp(Jet &J, u32 ratio_pct) {
             }
         } else {
             s32 bd = -1;
-            for (u32 b: J.touched) {
+            for (u32 b: C.touched) {
                 if (b == o) continue;
                 s32 delta = 0;
-                for (u32 id: J.touched) delta = wadd(delta, wmul(J.conn_of(id), wsub(J.dist(o, id), J.dist(b, id))));
+                for (u32 id: C.touched) delta = wadd(delta, wmul(C.of(id), wsub(J.dist(o, id), J.dist(b, id))));
                 if (delta > bd) {
                     bd = delta;
                     best = b;
@@ -507,7 +547,9 @@ std::vector<u32> jet_lp(Jet &J, u32 ratio_pct) {
             J.lock[u] = 0;
         }
     }
-    for (u32 u: cands) {  // afterburner
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (s64 ci = 0; ci < (s64) cands.size(); ++ci) {  // afterburner (writes lock[u] only)
+        const u32 u = cands[(size_t) ci];
         const s32 ug = J.gain1[u];
         const u32 ou = J.map[u], nu = J.dest_part[u];
         s32 change = 0;
@@ -590,20 +632,23 @@ std::vector<u32> rebalance_weak(Jet &J) {
     std::vector<u32> under;
     for (u32 b = 0; b < k; ++b)
         if (J.bw[b] < max_b_w) under.push_back(b);
-    std::vector<u32> cands, keys;
-    std::vector<s32> wts;
-    std::vector<s32> gain(n, 0);
-    for (u32 u = 0; u < n; ++u) {
+    // per vertex (all threads): target and mini-bucket key; then the
+    // candidates in ascending vertex id
+    std::vector<u32> keyv(n);
+    std::vector<u8> is_cand(n, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (s64 ui = 0; ui < (s64) n; ++ui) {
+        const u32 u = (u32) ui;
         const u32 o = J.map[u];
         u32 best = o;
         s32 gn = 0;
         const s32 vw = VW(g, u);
         if (J.bw[o] > lmax && 2 * (s64) vw < 3 * ((s64) J.bw[o] - (s64) opt)) {
-            J.conn(u);
+            const Conn &C = J.conn(u);
             s32 best_w = 0;
-            const s32 own = J.conn_of(o);
-            for (u32 b: J.touched) {
-                s32 c = J.conn_of(b);
+            const s32 own = C.of(o);
+            for (u32 b: C.touched) {
+                s32 c = C.of(b);
                 if (J.bw[b] < max_b_w && c > best_w) {
                     best = b;
                     best_w = c;
@@ -618,12 +663,18 @@ std::vector<u32> rebalance_weak(Jet &J) {
         J.dest_part[u] = best;
         if (o != best) {
             u32 gt = gain_bucket(gn, vw);
-            u32 key = (MAX_BUCKETS * o + gt) * sections + (u % sections);
-            cands.push_back(u);
-            keys.push_back(key);
-            wts.push_back(vw);
+            keyv[u] = (MAX_BUCKETS * o + gt) * sections + (u % sections);
+            is_cand[u] = 1;
         }
     }
+    std::vector<u32> cands, keys;
+    std::vector<s32> wts;
+    for (u32 u = 0; u < n; ++u)
+        if (is_cand[u]) {
+            cands.push_back(u);
+            keys.push_back(keyv[u]);
+            wts.push_back(VW(g, u));
+        }
     BucketOrder bo;
     bo.build(keys, wts);
     std::vector<u32> moves;
@@ -649,32 +700,40 @@ std::vector<u32> rebalance_strong(Jet &J) {
     s32 max_vwgt = INT32_MIN;  // find max size :377-385 (Max reducer identity)
     for (u32 b = 0; b < k; ++b)
         if (J.bw[b] < max_b_w && max_b_w - J.bw[b] > max_vwgt) max_vwgt = max_b_w - J.bw[b];
-    std::vector<u32> cands, keys;
-    std::vector<s32> wts;
-    for (u32 u = 0; u < n; ++u) {  // score_candidates :404-442
+    std::vector<u32> keyv(n);
+    std::vector<u8> is_cand(n, 0);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (s64 ui = 0; ui < (s64) n; ++ui) {  // score_candidates :404-442
+        const u32 u = (u32) ui;
         const u32 o = J.map[u];
         const s32 ow = J.bw[o];
         const s32 vw = VW(g, u);
         if (ow > lmax && (s64) vw <= 2 * (s64) max_vwgt && (s64) vw < 2 * ((s64) ow - (s64) opt)) {
-            J.conn(u);
-            const s32 own = J.conn_of(o);
+            const Conn &C = J.conn(u);
+            const s32 own = C.of(o);
             s32 count = 0, sum = 0;
-            for (u32 b: J.touched) {
+            for (u32 b: C.touched) {
                 if (b == o) continue;
                 if (J.bw[b] < max_b_w) {
-                    sum = wadd(sum, J.conn_of(b));
+                    sum = wadd(sum, C.of(b));
                     ++count;
                 }
             }
             if (count == 0) count = 1;
             s32 gn = wsub(sum / count, own);
             u32 gt = gain_bucket(gn, std::min<s32>(vw, ow - lmax));
-            u32 key = (MAX_BUCKETS * o + gt) * sections + (u % sections) + 1;
-            cands.push_back(u);
-            keys.push_back(key);
-            wts.push_back(vw);
+            keyv[u] = (MAX_BUCKETS * o + gt) * sections + (u % sections) + 1;
+            is_cand[u] = 1;
         }
     }
+    std::vector<u32> cands, keys;
+    std::vector<s32> wts;
+    for (u32 u = 0; u < n; ++u)
+        if (is_cand[u]) {
+            cands.push_back(u);
+            keys.push_back(keyv[u]);
+            wts.push_back(VW(g, u));
+        }
     BucketOrder bo;
     bo.build(keys, wts);
     std::vector<s64> evict_adjust(k, 0);
@@ -739,8 +798,10 @@ void perform_moves(Jet &J, const std::vector<u32> &moves, s64 &obj, s32 &maxw) {
     std::vector<u8> moving(J.n, 0);
     for (u32 u: moves)
         if (J.dest_part[u] != J.map[u]) moving[u] = 1;
-    s64 d = 0;
-    for (u32 u: moves) {
+    s64 d = 0;  // exact integer sum: the same in any order
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : d)
+    for (s64 mi = 0; mi < (s64) moves.size(); ++mi) {
+        const u32 u = moves[(size_t) mi];
         if (!moving[u]) continue;
         const u32 ou = J.map[u], nu = J.dest_part[u];
         for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
@@ -763,8 +824,14 @@ void perform_moves(Jet &J, const std::vector<u32> &moves, s64 &obj, s32 &maxw) {
         J.dest_part[u] = ou;
         J.dest_cache[u] = NULL_PART;
     }
-    for (u32 u: moves)
-        for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) J.dest_cache[g.adj[j]] = NULL_PART;
+#pragma omp parallel for schedule(dynamic, 256)
+    for (s64 mi = 0; mi < (s64) moves.size(); ++mi) {
+        const u32 u = moves[(size_t) mi];
+        for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
+#pragma omp atomic write
+            J.dest_cache[g.adj[j]] = NULL_PART;
+        }
+    }
     maxw = 0;
     for (u32 b = 0; b < J.k; ++b) maxw = std::max(maxw, J.bw[b]);
 }
@@ -918,6 +985,7 @@ const HostCSR &G(const void *g) { return *(const HostCSR *) g; }
 extern "C" {
 
 uint32_t or_xorshift32(uint32_t x) { return xorshift32(x); }
+int or_threads() { return omp_get_max_threads(); }
 uint32_t or_murmur3_u32(uint32_t key, uint32_t seed) { return murmur3_u32(key, seed); }
 uint32_t or_gain_bucket(int32_t gx, int32_t vwgt) { return gain_bucket(gx, vwgt); }
 uint32_t or_gain_bucket_float(int32_t gx, int32_t vwgt) { return gain_bucket_float(gx, vwgt); }

@@ -19,6 +19,7 @@ extern "C" {
 #endif
 
 // ---- hashes and scalar rules -------------------------------------------
+int or_threads(void);  // host threads the parallel loops use (OMP_NUM_THREADS)
 uint32_t or_xorshift32(uint32_t x);                 // two_hop_matching.h:93-100, graph.h:39-45
 uint32_t or_murmur3_u32(uint32_t key, uint32_t seed); // Kokkos::pod_hash<u32> (MurmurHash3_x86_32, 4-byte key)
 uint32_t or_gain_bucket(int32_t gx, int32_t vwgt);     // jet_label_propagation.h:147-180, exact integer rule

@@ -45,6 +45,7 @@ def lib():
     c = ctypes
     sig = {
         "or_xorshift32": (c.c_uint32, [c.c_uint32]),
+        "or_threads": (c.c_int, []),
         "or_murmur3_u32": (c.c_uint32, [c.c_uint32, c.c_uint32]),
         "or_gain_bucket": (c.c_uint32, [c.c_int32, c.c_int32]),
         "or_gain_bucket_float": (c.c_uint32, [c.c_int32, c.c_int32]),
@@ -237,6 +238,11 @@ def map_im(g, hier, dist, eps=0.03, seed=0):
     out = np.zeros(g.n, np.uint32)
     J = lib().or_map_im(g.h, _p(hier), _p(dist), len(hier), float(eps), int(seed), _p(out))
     return out, int(J)
+
+
+def threads():
+    """Host threads of the oracle's parallel loops (results do not depend on it)."""
+    return int(lib().or_threads())
 
 
 def xorshift32(x):
