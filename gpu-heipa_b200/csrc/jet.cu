@@ -404,17 +404,6 @@ __device__ __forceinline__ bool use_direct(const JArgs &a, u32 cap) {
     return a.k <= cap && (!a.code || a.k <= 256);
 }
 
-// Counts recomputed vertices / entries for roofline accounting.
-__device__ __forceinline__ void count_recompute(const JArgs &a, bool rec, u32 len) {
-    const unsigned mask = __ballot_sync(FULL, rec);
-    unsigned long long e = rec ? len : 0;
-    e = warp_sum<unsigned long long>(e);
-    if (lane_id() == 0 && mask) {
-        atomicAdd(&a.st->cnt[ST_AUX], (u32) __popc(mask));
-        atomicAdd((unsigned long long *) &a.st->sum[4], e);
-    }
-}
-
 // Tier of a row for the table-based kernels: 0 thread, 1 warp, 2 block.
 __device__ __forceinline__ int table_tier(u32 len, u32 k, u32 warp_max = JW_DEG) {
     if (len <= JT) return 0;
