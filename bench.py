@@ -236,6 +236,15 @@ def cpu_oracle_run(H, wl, args):
     return g.m // 2, time.perf_counter() - t0, obj, O.threads()
 
 
+def workload_config(wl, args, g, world):
+    """The `config` object of both arms' lines for a plain workload on graph g."""
+    h2d = 4 * (g.n + 1) + 4 * g.m + (4 * g.m if g.ew is not None else 0) + (4 * g.n if g.vw is not None else 0)
+    return {"workload": wl["desc"], "n": g.n, "undirected_edges": g.m // 2,
+            "k": wl["k"] if wl["task"] == "partition" else int(np.prod(wl["hier"])), "config": config_of(wl, args),
+            "seed": args.seed, "parallelism": f"replicas{world}",
+            "l2": "input CSR (%.2f GB) larger than L2 (126 MB)" % (h2d / 1e9)}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
@@ -249,11 +258,14 @@ def run_reference(args, world, rank):
             edges = e
     ms = 1000.0 * sum(times) / len(times)
     value = edges / (ms / 1000.0)
+    # the same config object as the GPU arm's line (the full workload's graph;
+    # each step times a bounded sample of it, named in cpu_baseline.sample)
+    config = workload_config(wl, args, make_graph(H, wl, args.seed), args.gpus)
     line = {
         "metric": "partition_throughput", "value": value, "unit": "edges/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": wl["desc"], "config": config_of(wl, args), "parallelism": "cpu"},
+        "config": config,
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": cores, "kind": "port", "sample": sample_desc(wl)},
         "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -518,10 +530,7 @@ def run_ours(args, world, rank, local):
         "metric": "partition_throughput", "value": value, "unit": "edges/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
-        "config": {"workload": wl["desc"], "n": g.n, "undirected_edges": edges,
-                   "k": wl["k"] if wl["task"] == "partition" else int(np.prod(wl["hier"])), "config": config_of(wl, args),
-                   "seed": args.seed, "parallelism": f"replicas{world}",
-                   "l2": "input CSR (%.2f GB) larger than L2 (126 MB)" % (h2d / 1e9)},
+        "config": workload_config(wl, args, g, world),
         "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms},
         "roofline": roofline,

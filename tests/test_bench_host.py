@@ -58,3 +58,6 @@ def test_reference_arm_under_torchrun():
         assert key in d, key
     assert d["value"] > 0 and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "port"
+    # the same config object as the GPU arm prints for this workload
+    assert d["config"]["n"] == 65536 and d["config"]["undirected_edges"] == 130560
+    assert d["config"]["k"] == 16 and d["config"]["parallelism"] == "replicas2"
