@@ -236,13 +236,25 @@ def cpu_oracle_run(H, wl, args):
     return g.m // 2, time.perf_counter() - t0, obj, O.threads()
 
 
+L2_BYTES = 126 << 20        # B200 L2
+L2_FLUSH_BYTES = 256 << 20  # written before every timed step when the input fits in L2
+
+
+def input_bytes(g):
+    return 4 * (g.n + 1) + 4 * g.m + (4 * g.m if g.ew is not None else 0) + (4 * g.n if g.vw is not None else 0)
+
+
 def workload_config(wl, args, g, world):
     """The `config` object of both arms' lines for a plain workload on graph g."""
-    h2d = 4 * (g.n + 1) + 4 * g.m + (4 * g.m if g.ew is not None else 0) + (4 * g.n if g.vw is not None else 0)
+    h2d = input_bytes(g)
+    if h2d > L2_BYTES:
+        l2 = "input CSR (%.2f GB) larger than L2 (126 MB)" % (h2d / 1e9)
+    else:
+        l2 = ("input CSR (%.1f MB) smaller than L2 (126 MB): a 256 MB buffer is written before every timed "
+              "step (L2 flush, inside the timed region)" % (h2d / 1e6))
     return {"workload": wl["desc"], "n": g.n, "undirected_edges": g.m // 2,
             "k": wl["k"] if wl["task"] == "partition" else int(np.prod(wl["hier"])), "config": config_of(wl, args),
-            "seed": args.seed, "parallelism": f"replicas{world}",
-            "l2": "input CSR (%.2f GB) larger than L2 (126 MB)" % (h2d / 1e9)}
+            "seed": args.seed, "parallelism": f"replicas{world}", "l2": l2}
 
 
 def run_reference(args, world, rank):
@@ -447,7 +459,19 @@ def run_ours(args, world, rank, local):
         ctx.tune(name, int(value))
     dg = ctx.upload(g)
     part = np.empty(g.n, np.uint32)
+    # inputs that fit in L2: write a buffer larger than L2 before every timed step
+    flush = None
+    if input_bytes(g) <= L2_BYTES:
+        import torch
+        flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def l2_flush():
+        if flush is not None:
+            flush.zero_()
+            torch.cuda.synchronize(local)
+
     for _ in range(args.warmup):
+        l2_flush()  # (the first one also loads the fill kernel)
         solve_device(ctx, dg, wl, args, part)
     sampler = ClockSampler(local)
     sampler.start()
@@ -458,6 +482,7 @@ def run_ours(args, world, rank, local):
     ctx.event_record(0)
     cuts = []
     for _ in range(args.steps):
+        l2_flush()
         cuts.append(solve_device(ctx, dg, wl, args, part))
     ctx.event_record(1)
     ms_total = ctx.event_elapsed(0, 1)
@@ -494,11 +519,12 @@ def run_ours(args, world, rank, local):
     barrier(world)
     ctx.event_record(2)
     for _ in range(e2e_steps):
+        l2_flush()
         solve_host(ctx, hg, wl, args, hpart)
     ctx.event_record(3)
     e2e_ms_total = ctx.event_elapsed(2, 3) if e2e_steps else 0.0
     barrier(world)
-    h2d = 4 * (g.n + 1) + 4 * g.m + (4 * g.m if g.ew is not None else 0) + (4 * g.n if g.vw is not None else 0)
+    h2d = input_bytes(g)
     d2h = 4 * g.n
     ctx.close()
 
