@@ -37,6 +37,8 @@ int main(int argc, char **argv) {
         {"--verbose-level", "", "Whether to print.", "1", ""},
         {"--seed", "", "Seed of the initial partitioner.", "0", ""},
         {"--device", "", "CUDA device.", "0", ""},
+        {"--deterministic", "", "Accepted for compatibility: every result is deterministic (same input, seed and "
+                                "config give the same output).", "", "", false, true},
     });
     if (argc == 1) {
         opt.help(argv[0]);

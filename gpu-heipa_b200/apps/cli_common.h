@@ -21,6 +21,7 @@ namespace cli {
 struct Option {
     std::string large_key, small_key, description, default_val, input;
     bool is_set = false;
+    bool is_switch = false;  // takes no value
 };
 
 class Options {
@@ -38,8 +39,12 @@ public:
             const std::string a = argv[i];
             for (Option &o: opts_) {
                 if (a == o.large_key || (!o.small_key.empty() && a == o.small_key)) {
-                    if (i + 1 >= argc) fail("missing value for " + a);
-                    o.input = argv[++i];
+                    if (o.is_switch) {
+                        o.input = "1";
+                    } else {
+                        if (i + 1 >= argc) fail("missing value for " + a);
+                        o.input = argv[++i];
+                    }
                     o.is_set = true;
                     break;
                 }

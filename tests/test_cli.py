@@ -34,6 +34,11 @@ def test_cli_help_and_argument_errors(tmp_path):
     # unreadable graph file
     r = _run([HEIPA, "-g", str(tmp_path / "missing.graph"), "-k", "4", "-c", "default"])
     assert r.returncode != 0 and "reading" in r.stderr
+    # --deterministic is a switch (takes no value) in both tools
+    for tool in (HEIPA, PROMAP):
+        assert "--deterministic" in _run([tool, "--help"]).stdout
+    r = _run([HEIPA, "--deterministic", "-g", str(tmp_path / "missing.graph"), "-k", "4", "-c", "default"])
+    assert r.returncode != 0 and "reading" in r.stderr
 
 
 def _stat(stdout, key):
