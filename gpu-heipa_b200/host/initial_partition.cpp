@@ -6,6 +6,8 @@
 #include <cmath>
 #include <numeric>
 
+#include <omp.h>
+
 namespace hp {
 namespace {
 
@@ -171,9 +173,9 @@ s64 overload(const s64 pw[2], const s64 maxw[2]) {
     return std::max<s64>(0, pw[0] - maxw[0]) + std::max<s64>(0, pw[1] - maxw[1]);
 }
 
-// Greedy graph growing: side 0 is grown from a random seed vertex until it
-// reaches target0.
-void grow_bisection(const IGraph &g, s64 target0, Rng64 &rng, std::vector<u8> &side) {
+// Greedy graph growing: side 0 is grown from the seed vertex `start` (drawn
+// at random by the caller, start < n) until it reaches target0.
+void grow_bisection(const IGraph &g, s64 target0, u32 start, std::vector<u8> &side) {
     const u32 n = g.n;
     side.assign(n, 1);
     if (n == 0) return;
@@ -186,8 +188,7 @@ void grow_bisection(const IGraph &g, s64 target0, Rng64 &rng, std::vector<u8> &s
     MaxHeap heap;
     heap.init(n);
     s64 w0 = 0;
-    u32 scan = rng.below(n);
-    u32 start = scan;
+    u32 scan = start;
     heap.push(start, gain[start]);
     u32 added = 0;
     while (w0 < target0 && added < n) {
@@ -334,6 +335,9 @@ void side_weights(const IGraph &g, const std::vector<u8> &side, s64 pw[2]) {
     for (u32 u = 0; u < g.n; ++u) pw[side[u]] += g.vw[u];
 }
 
+constexpr int BISECTION_TRIES = 8;
+thread_local int t_threads = BISECTION_TRIES;  // set_initial_partition_threads
+
 // Multilevel bisection with side 0 targeting `target0`.
 void multilevel_bisect(const IGraph &g, s64 target0, double ub, Rng64 &rng, std::vector<u8> &side) {
     const s64 maxw[2] = {(s64) std::floor((double) target0 * ub), (s64) std::floor((double) (g.W - target0) * ub)};
@@ -350,22 +354,33 @@ void multilevel_bisect(const IGraph &g, s64 target0, double ub, Rng64 &rng, std:
         cmaps.push_back(std::move(cmap));
         cur = &levels.back();
     }
-    // initial bisection on the coarsest level: best of several grown tries
-    std::vector<u8> best_side, try_side;
-    s64 best_cut = 0, best_ov = 0;
-    const int tries = 8;
-    for (int t = 0; t < tries; ++t) {
-        grow_bisection(*cur, target0, rng, try_side);
-        s64 pw[2];
-        side_weights(*cur, try_side, pw);
-        s64 c = fm_refine(*cur, try_side, pw, maxw, 4);
-        s64 ov = overload(pw, maxw);
-        if (t == 0 || ov < best_ov || (ov == best_ov && c < best_cut)) {
-            best_cut = c;
-            best_ov = ov;
-            best_side = try_side;
-        }
+    // initial bisection on the coarsest level: best of several grown tries.
+    // The seed vertices are drawn in order first; the tries are independent
+    // and run on up to t_threads host threads, and the best one is chosen in
+    // try order, so the result does not depend on the threads.
+    const int tries = BISECTION_TRIES;
+    if (cur->n == 0) {
+        side.assign(g.n, 1);
+        return;
     }
+    u32 starts[tries];
+    for (int t = 0; t < tries; ++t) starts[t] = rng.below(cur->n);
+    std::vector<u8> try_side[tries];
+    s64 try_cut[tries], try_ov[tries];
+    const int nt = std::max(1, std::min(tries, t_threads));
+#pragma omp parallel for num_threads(nt) schedule(static, 1) if (nt > 1)
+    for (int t = 0; t < tries; ++t) {
+        grow_bisection(*cur, target0, starts[t], try_side[t]);
+        s64 pw[2];
+        side_weights(*cur, try_side[t], pw);
+        try_cut[t] = fm_refine(*cur, try_side[t], pw, maxw, 4);
+        try_ov[t] = overload(pw, maxw);
+    }
+    int bt = 0;
+    for (int t = 1; t < tries; ++t)
+        if (try_ov[t] < try_ov[bt] || (try_ov[t] == try_ov[bt] && try_cut[t] < try_cut[bt])) bt = t;
+    std::vector<u8> best_side;
+    best_side.swap(try_side[bt]);
     // project and refine
     for (size_t li = levels.size(); li > 0; --li) {
         const IGraph &fine = (li >= 2) ? levels[li - 2] : g;
@@ -486,6 +501,8 @@ void kway_refine(const IGraph &g, u32 k, s64 lmax, std::vector<u32> &part, int p
 }
 
 } // namespace
+
+void set_initial_partition_threads(int threads) { t_threads = threads; }
 
 void initial_kway(const HostCSR &hg, u32 k, double eps, u64 seed, std::vector<u32> &part) {
     part.assign(hg.n, 0);

@@ -18,6 +18,12 @@ namespace hp {
 // eps and seed.
 void initial_kway(const HostCSR &g, u32 k, double eps, u64 seed, std::vector<u32> &part);
 
+// Host threads the initial partitioner may use on the calling thread (the
+// bisection tries of one coarsest level run concurrently); 1 = sequential.
+// Results do not depend on it. Threads that run concurrent sub-solves set 1
+// so that they do not oversubscribe the host. Default 8.
+void set_initial_partition_threads(int threads);
+
 // Imbalance for a sub-problem of a hierarchical split, as in
 // src/initial_partitioning/global_multisection.h:39-48.
 double adaptive_imbalance(double global_eps, s64 global_w, u32 global_k, s64 local_w, u32 local_k_rem, u64 depth);
