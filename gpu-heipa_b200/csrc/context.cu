@@ -1,6 +1,9 @@
 #include "context.h"
 
 #include <chrono>
+#include <condition_variable>
+#include <map>
+#include <mutex>
 
 namespace hp {
 
@@ -211,6 +214,32 @@ void Ctx::destroy() {
     d_status = nullptr;
     h_status = nullptr;
     stream = nullptr;
+}
+
+namespace {
+std::mutex g_coop_mu;
+std::condition_variable g_coop_cv;
+std::map<int, u32> g_coop_used;  // device -> SMs held by running cooperative grids
+}  // namespace
+
+u32 CoopSlots::acquire(int device, u32 sms, u32 sm_count) {
+    if (sm_count == 0) sm_count = 1;
+    if (sms > sm_count) sms = sm_count;
+    if (sms == 0) sms = 1;
+    std::unique_lock<std::mutex> lock(g_coop_mu);
+    u32 &used = g_coop_used[device];
+    g_coop_cv.wait(lock, [&] { return used + sms <= sm_count; });
+    used += sms;
+    return sms;
+}
+
+void CoopSlots::release(int device, u32 sms) {
+    {
+        std::lock_guard<std::mutex> lock(g_coop_mu);
+        u32 &used = g_coop_used[device];
+        used = used >= sms ? used - sms : 0;
+    }
+    g_coop_cv.notify_all();
 }
 
 void Ctx::zero_status() { HP_CUDA(cudaMemsetAsync(d_status, 0, sizeof(DevStatus), stream)); }

@@ -182,6 +182,37 @@ struct Ctx {
     }
 };
 
+// SMs held by cooperative launches (grids whose blocks wait for one another
+// at grid barriers) that run at the same time on one device. Concurrent
+// solves (HM sub-solves, batch and server requests) may each launch one; if
+// the grids together needed more SMs than the device has, blocks of one grid
+// could wait at its barrier for SMs held by waiting blocks of another, and
+// only the barrier's bounded wait would end that (with an error). A launch
+// therefore first takes ceil(blocks / blocks-per-SM) of the device's SMs here
+// (waiting on the host until they are free) and gives them back when its
+// kernel has finished, so all blocks of all running grids fit at once.
+class CoopSlots {
+public:
+    // Takes min(sms, sm_count) SMs of `device` (waits until free); returns them.
+    static u32 acquire(int device, u32 sms, u32 sm_count);
+    static void release(int device, u32 sms);
+};
+
+// Holds the SMs of one cooperative launch for the lifetime of the scope; the
+// scope must end after the kernel has completed (a stream synchronisation).
+struct CoopGuard {
+    int device;
+    u32 held;
+    CoopGuard(int dev, u32 blocks, u32 blocks_per_sm, u32 sm_count)
+        : device(dev),
+          held(CoopSlots::acquire(dev, (blocks + (blocks_per_sm ? blocks_per_sm : 1) - 1) /
+                                           (blocks_per_sm ? blocks_per_sm : 1),
+                                  sm_count)) {}
+    ~CoopGuard() { CoopSlots::release(device, held); }
+    CoopGuard(const CoopGuard &) = delete;
+    CoopGuard &operator=(const CoopGuard &) = delete;
+};
+
 // Records a CUDA-event pair around the launches in a C++ scope when
 // instrumentation is enabled (no synchronisation).
 struct KernTimer {

@@ -5,6 +5,7 @@
 #include "jet.cuh"
 
 #include <mutex>
+#include <optional>
 #include <vector>
 #include "prims.cuh"
 
@@ -2538,10 +2539,14 @@ static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &rati
     ctx.zero_counters();
     const size_t smem = 34 * (size_t) k * sizeof(s32);
     JArgs a = make_args(L);
+    std::optional<CoopGuard> coop;  // SMs of the cooperative grid, until the status read below
     if (blocks <= 1) {
         KernTimer kt(ctx, "k_jet_fused");
         k_jet_loop<false><<<1, FB, smem, ctx.stream>>>(a, F, d); note_launch();
     } else {
+        int per_sm = 1;
+        HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jet_loop<true>, FB, smem));
+        coop.emplace(ctx.device, blocks, (u32) std::max(per_sm, 1), (u32) ctx.sm_count);
         KernTimer kt(ctx, "k_jet_coop");
         void *args[] = {&a, &F, &d};
         HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_jet_loop<true>, dim3(blocks), dim3(FB), args, smem,

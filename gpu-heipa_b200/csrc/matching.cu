@@ -537,6 +537,8 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
         u32 cnt0 = n;
         u32 sd = seed;
         void *args[] = {&gg, &vcmap, &hn, &pl, &pl2, &cnt0, &claim, &heavy, &huge, &ctr, &sd, &bar, &err};
+        // SMs of this cooperative grid, held until the status read below
+        CoopGuard coop(ctx.device, grid, (u32) per_sm, (u32) ctx.sm_count);
         HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_match_loop, dim3(grid), dim3(PICK_BLOCK), args, 0,
                                             ctx.stream));
         note_launch();
