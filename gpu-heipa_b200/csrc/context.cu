@@ -219,25 +219,29 @@ void Ctx::destroy() {
 namespace {
 std::mutex g_coop_mu;
 std::condition_variable g_coop_cv;
-std::map<int, u32> g_coop_used;  // device -> SMs held by running cooperative grids
+std::map<int, bool> g_coop_taken;  // device -> a cooperative grid holds the slot
 }  // namespace
 
-u32 CoopSlots::acquire(int device, u32 sms, u32 sm_count) {
-    if (sm_count == 0) sm_count = 1;
-    if (sms > sm_count) sms = sm_count;
-    if (sms == 0) sms = 1;
+void CoopSlots::acquire(int device) {
     std::unique_lock<std::mutex> lock(g_coop_mu);
-    u32 &used = g_coop_used[device];
-    g_coop_cv.wait(lock, [&] { return used + sms <= sm_count; });
-    used += sms;
-    return sms;
+    bool &taken = g_coop_taken[device];
+    g_coop_cv.wait(lock, [&] { return !taken; });
+    taken = true;
 }
 
-void CoopSlots::release(int device, u32 sms) {
+bool CoopSlots::try_acquire_for(int device, int timeout_ms) {
+    std::unique_lock<std::mutex> lock(g_coop_mu);
+    bool &taken = g_coop_taken[device];
+    if (!g_coop_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms), [&] { return !taken; }))
+        return false;
+    taken = true;
+    return true;
+}
+
+void CoopSlots::release(int device) {
     {
         std::lock_guard<std::mutex> lock(g_coop_mu);
-        u32 &used = g_coop_used[device];
-        used = used >= sms ? used - sms : 0;
+        g_coop_taken[device] = false;
     }
     g_coop_cv.notify_all();
 }

@@ -182,36 +182,43 @@ struct Ctx {
     }
 };
 
-// SMs held by cooperative launches (grids whose blocks wait for one another
-// at grid barriers) that run at the same time on one device. Concurrent
-// solves (HM sub-solves, batch and server requests) may each launch one; if
-// the grids together needed more SMs than the device has, blocks of one grid
-// could wait at its barrier for SMs held by waiting blocks of another, and
-// only the barrier's bounded wait would end that (with an error). A launch
-// therefore first takes ceil(blocks / blocks-per-SM) of the device's SMs here
-// (waiting on the host until they are free) and gives them back when its
-// kernel has finished, so all blocks of all running grids fit at once.
+// Cooperative launches (grids whose blocks wait for one another at grid
+// barriers) run one at a time per device. Concurrent solves (HM sub-solves,
+// batch and server requests) may each want one; two such grids that were
+// each only partly resident (the block scheduler spreads blocks over all
+// SMs, next to kernels of other streams) could wait at their barriers for
+// SMs that the other's waiting blocks hold. With one cooperative grid per
+// device, every other kernel on the device finishes without waiting for it,
+// so its remaining blocks are always scheduled. A launch takes the device's
+// slot here (waiting on the host while another grid holds it) and returns it
+// after its kernel has completed.
 class CoopSlots {
 public:
-    // Takes min(sms, sm_count) SMs of `device` (waits until free); returns them.
-    static u32 acquire(int device, u32 sms, u32 sm_count);
-    static void release(int device, u32 sms);
+    static void acquire(int device);
+    // Waits at most timeout_ms; false when the slot stayed taken.
+    static bool try_acquire_for(int device, int timeout_ms);
+    static void release(int device);
 };
 
-// Holds the SMs of one cooperative launch for the lifetime of the scope; the
-// scope must end after the kernel has completed (a stream synchronisation).
+// Holds the device's cooperative slot for the lifetime of the scope. The
+// destructor first waits for `stream` (errors ignored), so the slot is never
+// returned while the grid may still run, even when the scope is left by an
+// exception between the launch and the status read.
 struct CoopGuard {
     int device;
-    u32 held;
-    CoopGuard(int dev, u32 blocks, u32 blocks_per_sm, u32 sm_count)
-        : device(dev),
-          held(CoopSlots::acquire(dev, (blocks + (blocks_per_sm ? blocks_per_sm : 1) - 1) /
-                                           (blocks_per_sm ? blocks_per_sm : 1),
-                                  sm_count)) {}
-    ~CoopGuard() { CoopSlots::release(device, held); }
+    cudaStream_t stream;
+    CoopGuard(int dev, cudaStream_t s) : device(dev), stream(s) { CoopSlots::acquire(dev); }
+    ~CoopGuard() {
+        cudaStreamSynchronize(stream);
+        CoopSlots::release(device);
+    }
     CoopGuard(const CoopGuard &) = delete;
     CoopGuard &operator=(const CoopGuard &) = delete;
 };
+
+// Thrown when a cooperative grid's bounded barrier wait gave up
+// (DEV_ERR_SPIN): the caller redoes that work on its per-kernel launch path.
+struct CoopSpin {};
 
 // Records a CUDA-event pair around the launches in a C++ scope when
 // instrumentation is enabled (no synchronisation).

@@ -2539,14 +2539,12 @@ static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &rati
     ctx.zero_counters();
     const size_t smem = 34 * (size_t) k * sizeof(s32);
     JArgs a = make_args(L);
-    std::optional<CoopGuard> coop;  // SMs of the cooperative grid, until the status read below
+    std::optional<CoopGuard> coop;  // the device's cooperative slot, until the kernel has completed
     if (blocks <= 1) {
         KernTimer kt(ctx, "k_jet_fused");
         k_jet_loop<false><<<1, FB, smem, ctx.stream>>>(a, F, d); note_launch();
     } else {
-        int per_sm = 1;
-        HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_jet_loop<true>, FB, smem));
-        coop.emplace(ctx.device, blocks, (u32) std::max(per_sm, 1), (u32) ctx.sm_count);
+        coop.emplace(ctx.device, ctx.stream);
         KernTimer kt(ctx, "k_jet_coop");
         void *args[] = {&a, &F, &d};
         HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_jet_loop<true>, dim3(blocks), dim3(FB), args, smem,
@@ -2556,7 +2554,7 @@ static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &rati
     HP_LAUNCH_CHECK();
     HP_CUDA(cudaMemcpyAsync(&h, d, sizeof(FusedCtl), cudaMemcpyDeviceToHost, ctx.stream));
     const DevStatus &st = ctx.read_status();
-    if (st.err & DEV_ERR_SPIN) throw HpError{HP_ERR_DEVICE, "Jet level loop: a grid barrier wait gave up"};
+    if (st.err & DEV_ERR_SPIN) throw CoopSpin{};
     if (st.err) throw HpError{HP_ERR_DEVICE, "Jet kernel reported error bits " + std::to_string(st.err)};
     obj = h.obj;
     maxw = h.maxw;
@@ -2601,8 +2599,22 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
             set_big_smem();
             const u32 blocks = coop_blocks(ctx, g.n, k);
             if (blocks) {
-                jet_refine_fused(ctx, L, ratios, promap, part, obj, maxw, blocks);
-                return;
+                // the level's input labelling, kept for the per-kernel path
+                // should the cooperative loop give up at a grid barrier
+                u32 *saved = ctx.balloc<u32>(g.n);
+                HP_CUDA(cudaMemcpyAsync(saved, part, sizeof(u32) * g.n, cudaMemcpyDeviceToDevice, ctx.stream));
+                const s64 obj0 = obj;
+                const s32 maxw0 = maxw;
+                try {
+                    jet_refine_fused(ctx, L, ratios, promap, part, obj, maxw, blocks);
+                    return;
+                } catch (const CoopSpin &) {
+                    HP_CUDA(cudaMemcpyAsync(part, saved, sizeof(u32) * g.n, cudaMemcpyDeviceToDevice, ctx.stream));
+                    ctx.zero_status();
+                    obj = obj0;
+                    maxw = maxw0;
+                    L.setup(ctx, g, k, lmax, D, part);
+                }
             }
         }
     }

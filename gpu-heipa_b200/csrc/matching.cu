@@ -493,10 +493,10 @@ u32 count_unmapped(Ctx &ctx, const u32 *vcmap, u32 n) {
 
 } // namespace
 
-u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
+// One matching of g into mapping; allow_coop selects the single cooperative
+// launch for the round loop of small levels.
+static u32 match_graph_impl(Ctx &ctx, const DGraph &g, u32 *mapping, bool allow_coop) {
     const u32 n = g.n;
-    if (n == 0) return 0;
-    ProfScope prof_all(ctx, "match");
     ScratchScope ss(ctx.arena);
     u32 *vcmap = ctx.balloc<u32>(n);
     u32 *hn = ctx.balloc<u32>(n);
@@ -523,7 +523,8 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
     // dominates) one cooperative launch, else one launch per phase with a
     // host read per round (large levels need more threads than fit at once)
     int per_sm = 0;
-    if (n <= std::min<u32>(ctx.tune.match_coop_max_n, MATCH_COOP_MAX_N) && g.m <= ctx.tune.match_coop_max_m)
+    if (allow_coop && n <= std::min<u32>(ctx.tune.match_coop_max_n, MATCH_COOP_MAX_N) &&
+        g.m <= ctx.tune.match_coop_max_m)
         HP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_match_loop, PICK_BLOCK, 0));
     if (per_sm > 0) {
         u32 *ctr = &ctx.d_status->cnt[8];  // 5 words, then the barrier's 2 words; cleared below
@@ -537,13 +538,13 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
         u32 cnt0 = n;
         u32 sd = seed;
         void *args[] = {&gg, &vcmap, &hn, &pl, &pl2, &cnt0, &claim, &heavy, &huge, &ctr, &sd, &bar, &err};
-        // SMs of this cooperative grid, held until the status read below
-        CoopGuard coop(ctx.device, grid, (u32) per_sm, (u32) ctx.sm_count);
+        // the device's cooperative slot, held until the kernel has completed
+        CoopGuard coop(ctx.device, ctx.stream);
         HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_match_loop, dim3(grid), dim3(PICK_BLOCK), args, 0,
                                             ctx.stream));
         note_launch();
         const DevStatus &st = ctx.read_status();
-        if (st.err & DEV_ERR_SPIN) throw HpError{HP_ERR_DEVICE, "matching loop: a grid barrier wait gave up"};
+        if (st.err & DEV_ERR_SPIN) throw CoopSpin{};
         if (st.cnt[12]) throw HpError{HP_ERR_DEVICE, "matching did not converge"};
     } else {
         u32 cnt = n;
@@ -645,6 +646,20 @@ u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
     k_final_map<<<ctx.grid(n, BLOCK), BLOCK, 0, ctx.stream>>>(vcmap, rank, mapping, n); note_launch();
     HP_LAUNCH_CHECK();
     return ctx.read_status().cnt[0];
+}
+
+u32 match_graph(Ctx &ctx, const DGraph &g, u32 *mapping) {
+    if (g.n == 0) return 0;
+    ProfScope prof_all(ctx, "match");
+    try {
+        return match_graph_impl(ctx, g, mapping, true);
+    } catch (const CoopSpin &) {
+        // the cooperative round loop gave up at a grid barrier: matching is
+        // a deterministic function of the graph, so redoing it from the
+        // start on the per-phase path gives the same mapping
+        ctx.zero_status();
+        return match_graph_impl(ctx, g, mapping, false);
+    }
 }
 
 } // namespace hp

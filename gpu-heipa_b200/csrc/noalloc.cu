@@ -81,10 +81,29 @@ bool on_device(const void *p, int dev) {
     return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
+// `part` is read on the host (copied into the scratch area), so device memory
+// there is a caller error.
+bool is_device_memory(const void *p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice;
+}
+
+// Every failing CUDA call leaves its error in the runtime's per-thread state;
+// clear it so that it is not reported later against the caller's own work.
+int cuda_failure() {
+    cudaGetLastError();
+    return HP_ERR_CUDA;
+}
+
 // One warp per vertex (grid-stride over warps). Every row and entry is bounds
-// checked against n and m: a row with xadj[u+1] < xadj[u] or xadj[u+1] > m, or
-// an entry with adj[e] >= n, is skipped and counted in counters[1], so bad
-// input yields an error status and never an out-of-range access.
+// checked against n and m: a row with xadj[u+1] < xadj[u] or xadj[u+1] > m, an
+// entry with adj[e] >= n, or an edge weight <= 0 (hp_graph_upload rejects the
+// same graphs) is skipped and counted in counters[1], so bad input yields an
+// error status and never an out-of-range access.
 __global__ void __launch_bounds__(kBlock)
 k_edge_cut_staged(uint32_t n, uint32_t m, const uint32_t *__restrict__ xadj, const uint32_t *__restrict__ adj,
                   const int32_t *__restrict__ ew, const uint32_t *__restrict__ part,
@@ -103,11 +122,12 @@ k_edge_cut_staged(uint32_t n, uint32_t m, const uint32_t *__restrict__ xadj, con
         const uint32_t pu = part[u];
         for (uint32_t e = beg + lane; e < end; e += 32) {
             const uint32_t v = adj[e];
-            if (v >= n) {
+            const int32_t w = ew ? ew[e] : 1;
+            if (v >= n || w <= 0) {
                 ++bad;
                 continue;
             }
-            if (part[v] != pu) acc += ew ? (long long) ew[e] : 1ll;
+            if (part[v] != pu) acc += (long long) w;
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -131,27 +151,31 @@ extern "C" int hp_edge_cut_noalloc(uint32_t n, uint32_t m, const uint32_t *d_xad
     if (dev < 0 || dev >= kMaxDevices) return HP_ERR_DEVICE;
     if (!on_device(d_xadj, dev) || (m > 0 && !on_device(d_adj, dev)) || (d_ew && !on_device(d_ew, dev)))
         return HP_ERR_ARG;
+    if (is_device_memory(part)) return HP_ERR_ARG;
     DeviceScratch s;
     const int rc = scratch_for_device(dev, &s);
-    if (rc != HP_OK) return rc;
+    if (rc != HP_OK) return rc == HP_ERR_CUDA ? cuda_failure() : rc;
 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned long long *counters = reinterpret_cast<unsigned long long *>(s.base);
     uint32_t *staged = reinterpret_cast<uint32_t *>(s.base + kHeadBytes);
-    if (cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st) != cudaSuccess) return HP_ERR_CUDA;
+    if (cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st) != cudaSuccess) return cuda_failure();
     if (n > 0) {
         if (cudaMemcpyAsync(staged, part, sizeof(uint32_t) * (size_t) n, cudaMemcpyHostToDevice, st) != cudaSuccess)
-            return HP_ERR_CUDA;
+            return cuda_failure();
         const uint64_t want = ((uint64_t) n * 32 + kBlock - 1) / kBlock;
         const uint64_t cap = (uint64_t) s.sms * kBlocksPerSm;
         const unsigned grid = (unsigned) (want < cap ? want : cap);
         k_edge_cut_staged<<<grid, kBlock, 0, st>>>(n, m, d_xadj, d_adj, d_ew, staged, counters);
-        if (cudaGetLastError() != cudaSuccess) return HP_ERR_CUDA;
+        if (cudaGetLastError() != cudaSuccess) return HP_ERR_CUDA;  // (cudaGetLastError cleared it)
     }
     unsigned long long host[2] = {0, 0};
-    if (cudaMemcpyAsync(host, counters, sizeof(host), cudaMemcpyDeviceToHost, st) != cudaSuccess) return HP_ERR_CUDA;
-    if (cudaStreamSynchronize(st) != cudaSuccess) return HP_ERR_CUDA;
+    if (cudaMemcpyAsync(host, counters, sizeof(host), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return cuda_failure();
+    if (cudaStreamSynchronize(st) != cudaSuccess) return cuda_failure();
     if (host[1] != 0) return HP_ERR_GRAPH;
-    *cut = (int64_t) (host[0] / 2);
+    // every accepted weight is positive, so the sum of directed entries is a
+    // non-negative int64; each undirected edge is counted twice
+    *cut = (int64_t) host[0] / 2;
     return HP_OK;
 }

@@ -9,6 +9,7 @@
 // involved.
 #include "../../include/gpuheipa.h"
 #include "common.cuh"
+#include "context.h"
 
 #include <cuda_runtime.h>
 
@@ -51,6 +52,7 @@ extern "C" int hp_selftest_barrier_timeout(int device, uint32_t blocks, uint32_t
         void *args[] = {&bar, &err, &absent};
         hp::u32 h_err = 0;
         float t = 0.f;
+        hp::CoopGuard coop(device, s);  // the device's cooperative slot, until the kernel has completed
         if (cudaMemsetAsync(d, 0, 4 * sizeof(hp::u32), s) != cudaSuccess || cudaEventRecord(e0, s) != cudaSuccess ||
             cudaLaunchCooperativeKernel((const void *) hp::k_barrier_selftest, dim3(blocks), dim3(32), args, 0, s) !=
                 cudaSuccess ||
@@ -69,4 +71,13 @@ extern "C" int hp_selftest_barrier_timeout(int device, uint32_t blocks, uint32_t
     if (e1) cudaEventDestroy(e1);
     if (s) cudaStreamDestroy(s);
     return rc;
+}
+
+extern "C" int hp_coop_slot_acquire(int device, int timeout_ms) {
+    return hp::CoopSlots::try_acquire_for(device, timeout_ms) ? HP_OK : HP_ERR_BUSY;
+}
+
+extern "C" int hp_coop_slot_release(int device) {
+    hp::CoopSlots::release(device);
+    return HP_OK;
 }

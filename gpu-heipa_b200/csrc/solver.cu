@@ -48,8 +48,9 @@ struct Hierarchy {
     std::vector<u32 *> maps;
 };
 
-// Coarsen while n > 8k (solver.h:343-347); stops early if a level makes no
-// progress.
+// Coarsen while n > 8k (solver.h:343-347); stops early when a matching
+// shrinks its level by less than 1% (the reference has no such check and
+// loops on graphs that stop coarsening; every level here costs arena space).
 void coarsen(Ctx &ctx, const DGraph &g, u32 k, Hierarchy &H, SolveStats *stats) {
     H.graphs.push_back(g);
     while (H.graphs.back().n > 8 * k) {
@@ -58,7 +59,7 @@ void coarsen(Ctx &ctx, const DGraph &g, u32 k, Hierarchy &H, SolveStats *stats) 
         u32 *mp = ctx.falloc<u32>(cur.n);
         const u32 nc = match_graph(ctx, cur, mp);
         if (stats) stats->coarsening_ms += ms_since(t0);
-        if (nc == cur.n) break;
+        if ((u64) nc * 100 > (u64) cur.n * 99) break;
         auto t1 = Clock::now();
         DGraph c = contract_graph(ctx, cur, mp, nc);
         if (stats) stats->contraction_ms += ms_since(t1);

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libgpuheipa.so")
 HP_MAP_IM, HP_MAP_HM, HP_MAP_HM_ULTRA = 0, 1, 2
 MAP_MODES = {"IM": HP_MAP_IM, "HM": HP_MAP_HM, "HM-ultra": HP_MAP_HM_ULTRA}
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "I/O error",
-          5: "invalid graph", 6: "device error", 7: "input too large"}
+          5: "invalid graph", 6: "device error", 7: "input too large", 8: "busy"}
 EDGE_CUT_NOALLOC_MAX_N = 4194304
 
 
@@ -61,6 +61,8 @@ _SIG = {
     "hp_comm_cost": (_int, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
     "hp_edge_cut_noalloc": (_int, [_u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hp_selftest_barrier_timeout": (_int, [ctypes.c_int, _u32, _vp, _vp]),
+    "hp_coop_slot_acquire": (_int, [ctypes.c_int, ctypes.c_int]),
+    "hp_coop_slot_release": (_int, [ctypes.c_int]),
     "hp_partition": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_partition_graph": (_int, [_vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_map": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
@@ -259,6 +261,21 @@ def kernel_launches():
 
 
 DEVERR_SPIN = 8  # device error bit: a bounded wait gave up
+
+
+def coop_slot_acquire(device=0, timeout_ms=0):
+    """Takes the device's cooperative-launch slot (hp_coop_slot_acquire).
+    Returns False when another holder kept it for timeout_ms."""
+    rc = _L.hp_coop_slot_acquire(device, int(timeout_ms))
+    if rc == 8:
+        return False
+    _host_check(rc, "cooperative slot acquire failed")
+    return True
+
+
+def coop_slot_release(device=0):
+    """Returns the device's cooperative-launch slot (hp_coop_slot_release)."""
+    _host_check(_L.hp_coop_slot_release(device), "cooperative slot release failed")
 
 
 def selftest_barrier_timeout(device=0, blocks=4):

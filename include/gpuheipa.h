@@ -32,7 +32,8 @@ enum {
     HP_ERR_IO = 4,
     HP_ERR_GRAPH = 5,
     HP_ERR_DEVICE = 6,
-    HP_ERR_TOO_LARGE = 7 /* input larger than a fixed-size entry point accepts */
+    HP_ERR_TOO_LARGE = 7, /* input larger than a fixed-size entry point accepts */
+    HP_ERR_BUSY = 8       /* a bounded wait for a shared resource timed out */
 };
 
 /* Mapping modes for hp_map / hp_map_graph (GPU-HeiProMap --config). */
@@ -128,9 +129,13 @@ int hp_comm_cost(hp_ctx *ctx, const hp_graph *g, const uint32_t *part, const uin
  * Limits and behaviour:
  *  - n > HP_EDGE_CUT_NOALLOC_MAX_N returns HP_ERR_TOO_LARGE before any device
  *    work; use hp_edge_cut for larger graphs.
- *  - Pointers that are not device memory of the current device return
- *    HP_ERR_ARG; rows with d_xadj[u+1] < d_xadj[u] or > m, or ids >= n, are
- *    skipped by the kernel and reported as HP_ERR_GRAPH.
+ *  - Graph pointers that are not device memory of the current device, or a
+ *    `part` in device memory, return HP_ERR_ARG; rows with d_xadj[u+1] <
+ *    d_xadj[u] or > m, ids >= n and edge weights <= 0 (the graphs that
+ *    hp_graph_upload rejects) are skipped by the kernel and reported as
+ *    HP_ERR_GRAPH.
+ *  - A failing CUDA call returns HP_ERR_CUDA with the runtime's error state
+ *    cleared, so it is not reported again against the caller's later work.
  *  - The first call on a device resolves the scratch address on that device
  *    (and loads the module there); make that first call before any stream
  *    capture begins. Later calls only read a table.
@@ -184,6 +189,19 @@ int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t
  * counterpart in the reference. */
 #define HP_DEVERR_SPIN 8u
 int hp_selftest_barrier_timeout(int device, uint32_t blocks, uint32_t *err_bits, double *ms);
+
+/* Diagnostics of the cooperative-launch slot (host only, no device work).
+ * Grids whose blocks wait for one another at grid barriers (the cooperative
+ * Jet level loop and matching loop, and the self-test above) run one at a
+ * time per device: each launch takes the device's slot and returns it after
+ * its kernel has completed, so two partly resident cooperative grids can
+ * never wait for each other. hp_coop_slot_acquire takes the slot of `device`
+ * (waiting at most timeout_ms; HP_ERR_BUSY when it stayed taken) and
+ * hp_coop_slot_release returns it; a caller that holds the slot delays every
+ * cooperative launch of this library on that device. No counterpart in the
+ * reference (it runs one solve on one stream). */
+int hp_coop_slot_acquire(int device, int timeout_ms);
+int hp_coop_slot_release(int device);
 
 /* Sets a size threshold that chooses between equivalent implementations
  * (results are identical; only the launch structure changes): "jet_graph_max_m"

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include <omp.h>
+#include <parallel/algorithm>
 
 #include "../gpu-heipa_b200/host/hp_types.h"
 #include "../gpu-heipa_b200/host/initial_partition.h"
@@ -44,6 +45,45 @@ inline s32 wadd(s32 a, s32 b) { return (s32) ((u32) a + (u32) b); }
 inline s32 wsub(s32 a, s32 b) { return (s32) ((u32) a - (u32) b); }
 inline s32 wmul(s32 a, s32 b) { return (s32) ((u32) a * (u32) b); }
 inline u32 deg(const HostCSR &g, u32 u) { return g.xadj[u + 1] - g.xadj[u]; }
+
+// The indices i in [0, n) with pred(i), ascending, selected on all host
+// threads (pred must be a pure function of i). Every loop below that the
+// reference runs as a filter or stable compaction uses it, so the order of
+// the result is the same as a one-thread scan.
+template<typename P>
+std::vector<u32> par_select(u32 n, P pred) {
+    const int T = omp_get_max_threads();
+    std::vector<size_t> cnt((size_t) T + 1, 0);
+    std::vector<u32> out;
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        const u32 lo = (u32) ((u64) n * (u64) t / (u64) nt), hi = (u32) ((u64) n * (u64) (t + 1) / (u64) nt);
+        size_t c = 0;
+        for (u32 i = lo; i < hi; ++i) c += pred(i) ? 1 : 0;
+        cnt[(size_t) t + 1] = c;
+#pragma omp barrier
+#pragma omp single
+        {
+            for (int i = 0; i < nt; ++i) cnt[(size_t) i + 1] += cnt[(size_t) i];
+            out.resize(cnt[(size_t) nt]);
+        }
+        size_t o = cnt[(size_t) t];
+        for (u32 i = lo; i < hi; ++i)
+            if (pred(i)) out[o++] = i;
+    }
+    return out;
+}
+
+// Relaxed atomic accesses for the few words that concurrent iterations of a
+// parallel loop share (results do not depend on the interleaving).
+inline u32 ld_relaxed(const u32 *p) { return __atomic_load_n(p, __ATOMIC_RELAXED); }
+inline void st_relaxed(u32 *p, u32 v) { __atomic_store_n(p, v, __ATOMIC_RELAXED); }
+inline void atomic_min_u32(u32 *p, u32 v) {
+    u32 cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+    while (v < cur && !__atomic_compare_exchange_n(p, &cur, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+    }
+}
 
 constexpr u32 N_MAX_ITERATIONS = 12;      // jet_label_propagation.h:36
 constexpr u32 N_MAX_WEAK_ITERATIONS = 2;  // jet_label_propagation.h:37
@@ -167,9 +207,12 @@ u32 pick(const HostCSR &g, const std::vector<u32> &vcmap, u32 u, u32 seed, bool 
 // matchHash two_hop_matching.h:205-253 under rule R2.
 template<typename D>
 void pair_by_digest(const std::vector<u32> &cands, const std::vector<D> &dig, std::vector<u32> &vcmap) {
+    // (digest, index) pairs are unique, so any sort gives the stable order
+    std::vector<std::pair<D, u32> > kv(cands.size());
+    for (size_t i = 0; i < cands.size(); ++i) kv[i] = {dig[i], (u32) i};
+    __gnu_parallel::sort(kv.begin(), kv.end());
     std::vector<u32> idx(cands.size());
-    std::iota(idx.begin(), idx.end(), 0u);
-    std::stable_sort(idx.begin(), idx.end(), [&](u32 a, u32 b) { return dig[a] < dig[b]; });
+    for (size_t i = 0; i < cands.size(); ++i) idx[i] = kv[i].second;
     size_t i = 0;
     while (i < idx.size()) {
         size_t j = i;
@@ -185,9 +228,10 @@ void pair_by_digest(const std::vector<u32> &cands, const std::vector<D> &dig, st
 }
 
 u32 count_unmapped(const std::vector<u32> &vcmap) {
-    u32 c = 0;
-    for (u32 x: vcmap) c += x == SENTINEL;
-    return c;
+    u64 c = 0;
+#pragma omp parallel for schedule(static) reduction(+ : c)
+    for (s64 i = 0; i < (s64) vcmap.size(); ++i) c += vcmap[(size_t) i] == SENTINEL;
+    return (u32) c;
 }
 
 u32 match(const HostCSR &g, std::vector<u32> &mapping) {
@@ -214,30 +258,48 @@ u32 match(const HostCSR &g, std::vector<u32> &mapping) {
     u32 round = 0;
     while (!list.empty()) {
         const u32 round_seed = seed ^ (round * 0x9e3779b1u);
+        const s64 L = (s64) list.size();
         for (u32 r = 0; r < 4; ++r) {
-            for (u32 u: list) {  // commit_p1
+#pragma omp parallel for schedule(static)
+            for (s64 li = 0; li < L; ++li) {  // commit_p1 (writes vcmap[u] of its own u only)
+                const u32 u = list[(size_t) li];
                 u32 v = hn[u];
                 if (v == SENTINEL || vcmap[u] != SENTINEL) continue;
                 bool cond = r > 0 ? (murmur3_u32(u + r, 0) < murmur3_u32(v + r, 0)) : (u < v);
                 if (!cond) vcmap[u] = SENTINEL - 1;
             }
-            std::vector<u32> touched;
-            for (u32 u: list) {  // commit_p2, rule R1
+            // commit_p2, rule R1: the smallest proposer of each receiver wins.
+            // Proposers (vcmap SENTINEL) and receivers (SENTINEL - 1) are
+            // disjoint and each proposer targets one receiver, so the pairs
+            // do not depend on the order in which they are written.
+#pragma omp parallel for schedule(static)
+            for (s64 li = 0; li < L; ++li) {
+                const u32 u = list[(size_t) li];
                 u32 v = hn[u];
                 if (v == SENTINEL || vcmap[u] != SENTINEL) continue;
                 if (vcmap[v] != SENTINEL - 1) continue;
-                if (claim[v] == SENTINEL) touched.push_back(v);
-                if (u < claim[v]) claim[v] = u;
+                atomic_min_u32(&claim[v], u);
             }
-            for (u32 v: touched) {
-                u32 u = claim[v];
+#pragma omp parallel for schedule(static)
+            for (s64 li = 0; li < L; ++li) {
+                const u32 u = list[(size_t) li];
+                u32 v = hn[u];
+                if (v == SENTINEL || ld_relaxed(&vcmap[u]) != SENTINEL || ld_relaxed(&claim[v]) != u) continue;
                 u32 cv = u < v ? u : v;
-                vcmap[v] = cv;
+                st_relaxed(&vcmap[v], cv);
                 vcmap[u] = cv;
-                claim[v] = SENTINEL;
             }
-            for (u32 u: list)  // commit_p3
+#pragma omp parallel for schedule(static)
+            for (s64 li = 0; li < L; ++li) {
+                const u32 u = list[(size_t) li];
+                u32 v = hn[u];
+                if (v != SENTINEL && ld_relaxed(&claim[v]) != SENTINEL) st_relaxed(&claim[v], SENTINEL);
+            }
+#pragma omp parallel for schedule(static)
+            for (s64 li = 0; li < L; ++li) {  // commit_p3
+                const u32 u = list[(size_t) li];
                 if (vcmap[u] == SENTINEL - 1) vcmap[u] = SENTINEL;
+            }
         }
 #pragma omp parallel for schedule(dynamic, 1024)
         for (s64 li = 0; li < (s64) list.size(); ++li) {  // re-pick (reads vcmap, writes hn[u] only)
@@ -245,10 +307,12 @@ u32 match(const HostCSR &g, std::vector<u32> &mapping) {
             if (vcmap[u] != SENTINEL || hn[u] == SENTINEL || vcmap[hn[u]] == SENTINEL) continue;
             hn[u] = pick(g, vcmap, u, round_seed, false);
         }
-        std::vector<u32> nl;  // compact
-        for (u32 u: list)
-            if (vcmap[u] == SENTINEL && hn[u] != SENTINEL) nl.push_back(u);
-        list.swap(nl);
+        std::vector<u32> keep = par_select((u32) list.size(), [&](u32 li) {  // compact
+            const u32 u = list[li];
+            return vcmap[u] == SENTINEL && hn[u] != SENTINEL;
+        });
+        for (u32 &x: keep) x = list[x];
+        list.swap(keep);
         ++round;
     }
     u32 unmapped = count_unmapped(vcmap);
@@ -265,26 +329,28 @@ u32 match(const HostCSR &g, std::vector<u32> &mapping) {
     }
     // twin matching: two_hop_matching.h:427-524
     if ((u64) unmapped * 4 > (u64) n) {
-        std::vector<u32> c;
-        std::vector<u64> d;
-        for (u32 i = 0; i < n; ++i) {
-            if (vcmap[i] != SENTINEL) continue;
+        std::vector<u32> c = par_select(n, [&](u32 i) { return vcmap[i] == SENTINEL; });
+        std::vector<u64> d(c.size());
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (s64 ci = 0; ci < (s64) c.size(); ++ci) {
+            const u32 i = c[(size_t) ci];
             u64 h = 0;
             for (u32 j = g.xadj[i]; j < g.xadj[i + 1]; ++j) {
                 u64 y = murmur3_u32(g.adj[j], 0);
                 h += y * y + y;
             }
-            c.push_back(i);
-            d.push_back(h);
+            d[(size_t) ci] = h;
         }
         pair_by_digest(c, d, vcmap);
         unmapped = count_unmapped(vcmap);
     }
     // relative matching: two_hop_matching.h:526-571, rule R3
     if ((u64) unmapped * 4 > (u64) n) {
-        std::vector<u32> c, d;
-        for (u32 i = 0; i < n; ++i) {
-            if (vcmap[i] != SENTINEL) continue;
+        std::vector<u32> c = par_select(n, [&](u32 i) { return vcmap[i] == SENTINEL; });
+        std::vector<u32> d(c.size());
+#pragma omp parallel for schedule(dynamic, 1024)
+        for (s64 ci = 0; ci < (s64) c.size(); ++ci) {
+            const u32 i = c[(size_t) ci];
             u32 h = SENTINEL;
             s32 max_wgt = 0;
             u32 min_deg = SENTINEL;
@@ -301,8 +367,7 @@ u32 match(const HostCSR &g, std::vector<u32> &mapping) {
                     max_wgt = w;
                 }
             }
-            c.push_back(i);
-            d.push_back(h);
+            d[(size_t) ci] = h;
         }
         pair_by_digest(c, d, vcmap);
     }
@@ -333,55 +398,60 @@ HostCSR contract(const HostCSR &g, const std::vector<u32> &mapping, u32 nc) {
         std::vector<u32> cur(moff.begin(), moff.end() - 1);
         for (u32 u = 0; u < g.n; ++u) mem[cur[mapping[u]]++] = u;
     }
-    // coarse rows on all threads, each with its own accumulator: pass 0
-    // counts the distinct neighbours of every coarse vertex, pass 1 writes the
-    // sorted rows at their offsets
+    // coarse rows on all threads, each with its own accumulator: every
+    // thread writes the sorted rows of its coarse vertices into its own
+    // buffer, then the rows are copied to their offsets
     c.xadj.assign(nc + 1, 0);
-    for (int pass = 0; pass < 2; ++pass) {
-        if (pass == 1) {
-            for (u32 i = 0; i < nc; ++i) c.xadj[i + 1] += c.xadj[i];
-            c.m = c.xadj[nc];
-            c.adj.resize(c.m);
-            c.ew.resize(c.m);
-        }
-#pragma omp parallel
-        {
-            std::vector<s32> acc(nc, 0);
-            std::vector<u8> seen(nc, 0);
-            std::vector<u32> touched;
+    const int T = omp_get_max_threads();
+    std::vector<std::vector<u32> > badj((size_t) T);
+    std::vector<std::vector<s32> > bew((size_t) T);
+    std::vector<u64> where(nc);  // (thread << 40) | offset in that thread's buffer
+#pragma omp parallel num_threads(T)
+    {
+        const int t = omp_get_thread_num();
+        std::vector<s32> acc(nc, 0);
+        std::vector<u8> seen(nc, 0);
+        std::vector<u32> touched;
+        std::vector<u32> &ba = badj[(size_t) t];
+        std::vector<s32> &be = bew[(size_t) t];
 #pragma omp for schedule(dynamic, 256)
-            for (s64 ci = 0; ci < (s64) nc; ++ci) {
-                const u32 cu = (u32) ci;
-                touched.clear();
-                for (u32 t = moff[cu]; t < moff[cu + 1]; ++t) {
-                    u32 u = mem[t];
-                    for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
-                        u32 cv = mapping[g.adj[j]];
-                        if (cv == cu) continue;
-                        if (!seen[cv]) {
-                            seen[cv] = 1;
-                            touched.push_back(cv);
-                        }
-                        acc[cv] = wadd(acc[cv], EW(g, j));
+        for (s64 ci = 0; ci < (s64) nc; ++ci) {
+            const u32 cu = (u32) ci;
+            touched.clear();
+            for (u32 q = moff[cu]; q < moff[cu + 1]; ++q) {
+                u32 u = mem[q];
+                for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
+                    u32 cv = mapping[g.adj[j]];
+                    if (cv == cu) continue;
+                    if (!seen[cv]) {
+                        seen[cv] = 1;
+                        touched.push_back(cv);
                     }
-                }
-                if (pass == 0) {
-                    c.xadj[cu + 1] = (u32) touched.size();
-                } else {
-                    std::sort(touched.begin(), touched.end());
-                    u32 o = c.xadj[cu];
-                    for (u32 cv: touched) {
-                        c.adj[o] = cv;
-                        c.ew[o] = acc[cv];
-                        ++o;
-                    }
-                }
-                for (u32 cv: touched) {
-                    acc[cv] = 0;
-                    seen[cv] = 0;
+                    acc[cv] = wadd(acc[cv], EW(g, j));
                 }
             }
+            std::sort(touched.begin(), touched.end());
+            where[cu] = ((u64) t << 40) | (u64) ba.size();
+            c.xadj[cu + 1] = (u32) touched.size();
+            for (u32 cv: touched) {
+                ba.push_back(cv);
+                be.push_back(acc[cv]);
+                acc[cv] = 0;
+                seen[cv] = 0;
+            }
         }
+    }
+    for (u32 i = 0; i < nc; ++i) c.xadj[i + 1] += c.xadj[i];
+    c.m = c.xadj[nc];
+    c.adj.resize(c.m);
+    c.ew.resize(c.m);
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (s64 ci = 0; ci < (s64) nc; ++ci) {
+        const u32 cu = (u32) ci;
+        const size_t t = (size_t) (where[cu] >> 40), off = (size_t) (where[cu] & ((1ull << 40) - 1));
+        const u32 len = c.xadj[cu + 1] - c.xadj[cu];
+        std::copy_n(badj[t].data() + off, len, c.adj.data() + c.xadj[cu]);
+        std::copy_n(bew[t].data() + off, len, c.ew.data() + c.xadj[cu]);
     }
     return c;
 }
@@ -432,7 +502,8 @@ s32 lmax_of(s64 W, u32 k, double eps) { return (s32) std::ceil((1.0 + eps) * ((d
 // ---------------------------------------------------------------------------
 
 // Connectivity row of one vertex (rule R7: the blocks adjacent to u with
-// their connection weight, ascending id). One per thread: the per-vertex
+// their connection weight, in first-seen order; every consumer breaks ties
+// by the lowest block id explicitly). One per thread: the per-vertex
 // loops of the Jet steps below read only state that the loop does not write,
 // so they run on all host threads with the same results as one thread.
 struct Conn {
@@ -446,7 +517,6 @@ struct Conn {
             if (acc[b] == 0) touched.push_back(b);
             acc[b] = wadd(acc[b], EW(g, j));
         }
-        std::sort(touched.begin(), touched.end());
     }
     s32 of(u32 b) const { return acc[b]; }
 };
@@ -461,6 +531,7 @@ struct Jet {
     std::vector<u32> map, dest_cache, dest_part, lock;
     std::vector<s32> bw, gain_cache, gain1;
     std::vector<Conn> conns;  // one per host thread
+    std::vector<u8> moving;   // perform_moves scratch, all zero between calls
 
     s32 dist(u32 a, u32 b) const { return D[(size_t) a * k + b]; }
     Conn &conn(u32 u) {
@@ -485,6 +556,7 @@ void jet_init(Jet &J, const HostCSR &g, u32 k, s32 lmax, const u32 *part) {
     J.dest_part.assign(g.n, NO_MOVE);
     J.lock.assign(g.n, 0);
     J.gain1.assign(g.n, 0);
+    J.moving.assign(g.n, 0);
     J.conns.assign((size_t) omp_get_max_threads(), Conn{});
     for (Conn &c: J.conns) c.acc.assign(k, 0);
 }
@@ -511,7 +583,7 @@ std::vector<u32> jet_lp(Jet &J, u32 ratio_pct) {
             for (u32 b: C.touched) {
                 if (b == o) continue;
                 s32 c = C.of(b);
-                if (c > bc) {
+                if (c > bc || (c == bc && best != NO_MOVE && b < best)) {  // rule R4
                     bc = c;
                     best = b;
                 }
@@ -526,7 +598,7 @@ std::vector<u32> jet_lp(Jet &J, u32 ratio_pct) {
                 if (b == o) continue;
                 s32 delta = 0;
                 for (u32 id: C.touched) delta = wadd(delta, wmul(C.of(id), wsub(J.dist(o, id), J.dist(b, id))));
-                if (delta > bd) {
+                if (delta > bd || (delta == bd && best != NO_MOVE && b < best)) {  // rule R4
                     bd = delta;
                     best = b;
                 }
@@ -537,16 +609,19 @@ std::vector<u32> jet_lp(Jet &J, u32 ratio_pct) {
         J.dest_cache[u] = best;
         J.dest_part[u] = best;
     }
-    std::vector<u32> cands;
-    for (u32 u = 0; u < n; ++u) {  // filter potentially viable moves
-        if (J.dest_part[u] != NO_MOVE && J.lock[u] == 0) {
-            cands.push_back(u);
+    std::vector<u8> viable(n);
+#pragma omp parallel for schedule(static)
+    for (s64 ui = 0; ui < (s64) n; ++ui) {  // filter potentially viable moves
+        const u32 u = (u32) ui;
+        viable[u] = J.dest_part[u] != NO_MOVE && J.lock[u] == 0;
+        if (viable[u]) {
             J.gain1[u] = J.gain_cache[u];
         } else {
             J.gain1[u] = GAIN_MIN;
             J.lock[u] = 0;
         }
     }
+    std::vector<u32> cands = par_select(n, [&](u32 u) { return viable[u] != 0; });
 #pragma omp parallel for schedule(dynamic, 1024)
     for (s64 ci = 0; ci < (s64) cands.size(); ++ci) {  // afterburner (writes lock[u] only)
         const u32 u = cands[(size_t) ci];
@@ -571,9 +646,8 @@ std::vector<u32> jet_lp(Jet &J, u32 ratio_pct) {
         }
         if (wadd(ug, change) >= 0) J.lock[u] = 1;
     }
-    std::vector<u32> moves;
-    for (u32 u: cands)
-        if (J.lock[u]) moves.push_back(u);
+    std::vector<u32> moves = par_select((u32) cands.size(), [&](u32 ci) { return J.lock[cands[ci]] != 0; });
+    for (u32 &x: moves) x = cands[x];
     return moves;
 }
 
@@ -596,18 +670,22 @@ struct BucketOrder {
     std::vector<s64> prefix;         // per candidate index
     void build(const std::vector<u32> &keys, const std::vector<s32> &w) {
         const size_t c = keys.size();
-        std::vector<u32> idx(c);
-        std::iota(idx.begin(), idx.end(), 0u);
-        std::stable_sort(idx.begin(), idx.end(), [&](u32 a, u32 b) { return keys[a] < keys[b]; });
+        // (key, candidate index) is unique, so sorting it gives the stable
+        // order by key
+        std::vector<u64> kv(c);
+#pragma omp parallel for schedule(static)
+        for (s64 i = 0; i < (s64) c; ++i) kv[(size_t) i] = ((u64) keys[(size_t) i] << 32) | (u64) i;
+        __gnu_parallel::sort(kv.begin(), kv.end());
         keys_sorted.resize(c);
         prefix_sorted.resize(c + 1);
         prefix.resize(c);
         s64 run = 0;
         for (size_t i = 0; i < c; ++i) {
-            keys_sorted[i] = keys[idx[i]];
+            const u32 id = (u32) kv[i];
+            keys_sorted[i] = (u32) (kv[i] >> 32);
             prefix_sorted[i] = run;
-            prefix[idx[i]] = run;
-            run += w[idx[i]];
+            prefix[id] = run;
+            run += w[id];
         }
         prefix_sorted[c] = run;
     }
@@ -617,6 +695,19 @@ struct BucketOrder {
         return prefix_sorted[pos];
     }
 };
+
+// The flagged vertices in ascending id with their keys and weights.
+void collect_candidates(const HostCSR &g, const std::vector<u8> &is_cand, const std::vector<u32> &keyv,
+                        std::vector<u32> &cands, std::vector<u32> &keys, std::vector<s32> &wts) {
+    cands = par_select(g.n, [&](u32 u) { return is_cand[u] != 0; });
+    keys.resize(cands.size());
+    wts.resize(cands.size());
+#pragma omp parallel for schedule(static)
+    for (s64 i = 0; i < (s64) cands.size(); ++i) {
+        keys[(size_t) i] = keyv[cands[(size_t) i]];
+        wts[(size_t) i] = VW(g, cands[(size_t) i]);
+    }
+}
 
 // rebalance_weak jet_label_propagation.h:592-751 (ProMap variant
 // promap_jet_label_propagation.h:554-717 computes the same move set).
@@ -649,7 +740,7 @@ std::vector<u32> rebalance_weak(Jet &J) {
             const s32 own = C.of(o);
             for (u32 b: C.touched) {
                 s32 c = C.of(b);
-                if (J.bw[b] < max_b_w && c > best_w) {
+                if (J.bw[b] < max_b_w && (c > best_w || (c == best_w && best != o && b < best))) {  // rule R4
                     best = b;
                     best_w = c;
                 }
@@ -669,21 +760,16 @@ std::vector<u32> rebalance_weak(Jet &J) {
     }
     std::vector<u32> cands, keys;
     std::vector<s32> wts;
-    for (u32 u = 0; u < n; ++u)
-        if (is_cand[u]) {
-            cands.push_back(u);
-            keys.push_back(keyv[u]);
-            wts.push_back(VW(g, u));
-        }
+    collect_candidates(g, is_cand, keyv, cands, keys, wts);
     BucketOrder bo;
     bo.build(keys, wts);
-    std::vector<u32> moves;
-    for (size_t i = 0; i < cands.size(); ++i) {
+    std::vector<u32> moves = par_select((u32) cands.size(), [&](u32 i) {
         u32 u = cands[i], o = J.map[u];
         s64 score = bo.prefix[i] - bo.B((u64) o * width);
         s64 limit = (s64) J.bw[o] - lmax;
-        if (score < limit) moves.push_back(u);
-    }
+        return score < limit;
+    });
+    for (u32 &x: moves) x = cands[x];
     return moves;
 }
 
@@ -728,20 +814,19 @@ std::vector<u32> rebalance_strong(Jet &J) {
     }
     std::vector<u32> cands, keys;
     std::vector<s32> wts;
-    for (u32 u = 0; u < n; ++u)
-        if (is_cand[u]) {
-            cands.push_back(u);
-            keys.push_back(keyv[u]);
-            wts.push_back(VW(g, u));
-        }
+    collect_candidates(g, is_cand, keyv, cands, keys, wts);
     BucketOrder bo;
     bo.build(keys, wts);
     std::vector<s64> evict_adjust(k, 0);
     std::vector<u32> moves;
     std::vector<s64> mscore;
+    std::vector<s64> scores(cands.size());
+#pragma omp parallel for schedule(static)
+    for (s64 i = 0; i < (s64) cands.size(); ++i)
+        scores[(size_t) i] = bo.prefix[(size_t) i] - bo.B((u64) J.map[cands[(size_t) i]] * width);
     for (size_t i = 0; i < cands.size(); ++i) {  // filter_scores :490-509
         u32 u = cands[i], o = J.map[u];
-        s64 score = bo.prefix[i] - bo.B((u64) o * width);
+        s64 score = scores[i];
         s64 limit = (s64) J.bw[o] - lmax;
         if (score < limit) {
             if (score + VW(g, u) >= limit) evict_adjust[o] = score + VW(g, u);
@@ -795,9 +880,13 @@ std::vector<u32> rebalance_strong(Jet &J) {
 // cut = directed/2, J = directed).
 void perform_moves(Jet &J, const std::vector<u32> &moves, s64 &obj, s32 &maxw) {
     const HostCSR &g = *J.g;
-    std::vector<u8> moving(J.n, 0);
-    for (u32 u: moves)
+    std::vector<u8> &moving = J.moving;
+    const s64 M = (s64) moves.size();
+#pragma omp parallel for schedule(static)
+    for (s64 mi = 0; mi < M; ++mi) {
+        const u32 u = moves[(size_t) mi];
         if (J.dest_part[u] != J.map[u]) moving[u] = 1;
+    }
     s64 d = 0;  // exact integer sum: the same in any order
 #pragma omp parallel for schedule(dynamic, 256) reduction(+ : d)
     for (s64 mi = 0; mi < (s64) moves.size(); ++mi) {
@@ -815,21 +904,34 @@ void perform_moves(Jet &J, const std::vector<u32> &moves, s64 &obj, s32 &maxw) {
         }
     }
     obj += J.promap ? d : d / 2;
-    for (u32 u: moves) {
-        const u32 ou = J.map[u], nu = J.dest_part[u];
-        const s32 w = VW(g, u);
-        J.bw[ou] = wsub(J.bw[ou], w);
-        J.bw[nu] = wadd(J.bw[nu], w);
-        J.map[u] = nu;
-        J.dest_part[u] = ou;
-        J.dest_cache[u] = NULL_PART;
+    // block weights: per-thread wrapping s32 deltas (the sum is the same in
+    // any order); labels: one vertex per iteration
+    const int T = omp_get_max_threads();
+    std::vector<s32> bwd((size_t) T * J.k, 0);
+#pragma omp parallel num_threads(T)
+    {
+        s32 *dk = bwd.data() + (size_t) omp_get_thread_num() * J.k;
+#pragma omp for schedule(static)
+        for (s64 mi = 0; mi < M; ++mi) {
+            const u32 u = moves[(size_t) mi];
+            const u32 ou = J.map[u], nu = J.dest_part[u];
+            const s32 w = VW(g, u);
+            dk[ou] = wsub(dk[ou], w);
+            dk[nu] = wadd(dk[nu], w);
+            J.map[u] = nu;
+            J.dest_part[u] = ou;
+            J.dest_cache[u] = NULL_PART;
+            moving[u] = 0;
+        }
     }
+    for (int t = 0; t < T; ++t)
+        for (u32 b = 0; b < J.k; ++b) J.bw[b] = wadd(J.bw[b], bwd[(size_t) t * J.k + b]);
 #pragma omp parallel for schedule(dynamic, 256)
     for (s64 mi = 0; mi < (s64) moves.size(); ++mi) {
         const u32 u = moves[(size_t) mi];
         for (u32 j = g.xadj[u]; j < g.xadj[u + 1]; ++j) {
-#pragma omp atomic write
-            J.dest_cache[g.adj[j]] = NULL_PART;
+            u32 *dc = &J.dest_cache[g.adj[j]];
+            if (ld_relaxed(dc) != NULL_PART) st_relaxed(dc, NULL_PART);  // skip shared lines already reset
         }
     }
     maxw = 0;
@@ -930,7 +1032,7 @@ s64 partition_graph(const HostCSR &g, u32 k, double eps, bool ultra, u64 seed, s
     while (cur->n > 8 * k) {  // solver.h:343-347
         std::vector<u32> mapping;
         u32 nc = match(*cur, mapping);
-        if (nc == cur->n) break;  // no progress: stop coarsening
+        if ((u64) nc * 100 > (u64) cur->n * 99) break;  // shrank by less than 1%: stop coarsening
         graphs.push_back(contract(*cur, mapping, nc));
         maps.push_back(std::move(mapping));
         cur = &graphs.back();
@@ -1150,7 +1252,7 @@ int64_t or_map_im(const void *gp, const uint32_t *hier, const int32_t *dist, uin
     while (cur->n > 8 * k) {  // promap_solver.h:247-251
         std::vector<u32> mapping;
         u32 nc = match(*cur, mapping);
-        if (nc == cur->n) break;
+        if ((u64) nc * 100 > (u64) cur->n * 99) break;  // shrank by less than 1%
         graphs.push_back(contract(*cur, mapping, nc));
         maps.push_back(std::move(mapping));
         cur = &graphs.back();

@@ -5,7 +5,9 @@ import numpy as np
 import pytest
 
 import gpu_heipa as H
+import oracle as O
 from conftest import has_gpu
+from helpers import to_oracle
 
 
 def _mix():
@@ -23,6 +25,9 @@ def test_batch_equals_plain(ctx):
         want, wcut = ctx.partition(g, k, 0.03, "default", 1)
         np.testing.assert_array_equal(part, want)
         assert cut == wcut
+        opart, ocut = O.partition(to_oracle(g), k, 0.03, False, 1)
+        np.testing.assert_array_equal(part, opart)
+        assert cut == ocut
 
 
 @pytest.mark.gpu

@@ -1,7 +1,8 @@
 """hp_edge_cut_noalloc: the edge cut of a caller-owned device CSR computed in
-a fixed static scratch area, checked against the arena-backed hp_edge_cut on
-the same graph and partitions, two calls in a row. The graph arrays live in
-PyTorch CUDA tensors, i.e. in memory the library does not own.
+a fixed static scratch area, checked against the arena-backed hp_edge_cut and
+against the CPU oracle's edge_cut on the same graph and partitions, two calls
+in a row. The graph arrays live in PyTorch CUDA tensors, i.e. in memory the
+library does not own.
 
 This file is named to be collected last, so the entry point also runs after
 every other GPU test has used the library on the same device."""
@@ -9,6 +10,7 @@ import numpy as np
 import pytest
 
 import gpu_heipa as H
+import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -43,10 +45,12 @@ def test_noalloc_matches_edge_cut_two_calls(ctx, gname):
         parts = [rng.integers(0, 16, g.n, dtype=np.uint32), rng.integers(0, 64, g.n, dtype=np.uint32)]
         side = torch.cuda.Stream()
         streams = [0, side.cuda_stream]  # first call on the default stream, second on a side stream
+        og = O.Graph(g.xadj, g.adj, g.ew, g.vw)
         for part, st in zip(parts, streams):
             got = H.edge_cut_noalloc(g.n, g.m, px, pa, pw, part, stream=st)
-            want = ctx.edge_cut(dg, part)
+            want = O.edge_cut(og, part)
             assert got == want
+            assert ctx.edge_cut(dg, part) == want
             assert got > 0
         # A partition with every vertex in one block has no cut.
         assert H.edge_cut_noalloc(g.n, g.m, px, pa, pw, np.zeros(g.n, np.uint32)) == 0
@@ -79,9 +83,26 @@ def test_noalloc_rejects_bad_input(ctx):
         H.edge_cut_noalloc(g.n, g.m, px, bad.data_ptr(), pw, part)
     assert e.value.code == 5
 
+    # A negative edge weight: rejected like hp_graph_upload rejects it.
+    neg = ew.clone()
+    neg[7] = -3
+    with pytest.raises(H.HeiPaError) as e:
+        H.edge_cut_noalloc(g.n, g.m, px, pa, neg.data_ptr(), part)
+    assert e.value.code == 5
+
+    # The partition must be host memory: a device pointer is refused (raw C
+    # ABI call; the Python wrapper only takes host arrays).
+    import ctypes
+    import torch
+    dpart = torch.from_numpy(part.view(np.int32).copy()).cuda()
+    out = ctypes.c_int64(-1)
+    rc = H._L.hp_edge_cut_noalloc(g.n, g.m, px, pa, pw, ctypes.c_void_p(dpart.data_ptr()), None, ctypes.byref(out))
+    assert rc == 1 and out.value == -1
+
     # The scratch counters are cleared by every call: a good call after the
     # failures gives the same result as before.
     assert H.edge_cut_noalloc(g.n, g.m, px, pa, pw, part) == want
+    assert want == O.edge_cut(O.Graph(g.xadj, g.adj, g.ew, g.vw), part)
     dg = ctx.upload(g)
     try:
         assert want == ctx.edge_cut(dg, part)
