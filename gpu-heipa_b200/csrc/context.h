@@ -137,6 +137,7 @@ struct Tunables {
     u32 jet_coop_max_deg = 32;         // ... and average degree (dense levels keep the whole GPU)
     u32 jet_coop_rows = 1024;          // vertices per block of that grid
     u32 jet_hub_deg = 1024;            // Jet table passes: rows above this length are cut into chunks of it (64..4096)
+    u32 jet_chunk_mode = 0;            // chunk kernels: 0 = 4 entries per lane, 1 = 8, 2 = bulk-copy staged rows
 };
 
 struct Ctx {

@@ -3,6 +3,7 @@
 // tie rules documented in jet.cuh (lowest block id on best-block ties,
 // mini-bucket order by vertex id, fallback slots in ascending vertex id).
 #include "jet.cuh"
+#include "stage.cuh"
 
 #include <mutex>
 #include <optional>
@@ -710,7 +711,39 @@ __global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
 // are read through the non-coherent path; four entries per thread are loaded
 // (ids, then labels, then old labels of moved neighbours) before the cache
 // resets are stored, which keeps four dependent gathers in flight.
-template<bool NC = true>
+// Objective contribution and cache resets of B loaded entries (v = SENTINEL
+// marks an empty slot) of a row whose vertex has new label nu and old label
+// ou (um: it changed block). All B labels are gathered, then the old labels
+// of moved neighbours, so B dependent gathers are in flight at a time.
+template<int B, bool NC>
+__device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou, bool um, const u32 (&v)[B],
+                                                 const s32 (&w)[B], bool inval) {
+    long long acc = 0;
+    if (um) {
+        u32 xv[B], ov[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) xv[j] = v[j] != SENTINEL ? ldj<NC>(&a.map[v[j]]) : 0;
+#pragma unroll
+        for (int j = 0; j < B; ++j) ov[j] = (xv[j] & MOVED) ? ldj<NC>(&a.dest_part[v[j]]) : (xv[j] & ~MOVED);
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            if (v[j] == SENTINEL) continue;
+            const u32 nv = xv[j] & ~MOVED;
+            long long c;
+            if (!a.code) c = (long long) w[j] * ((long long) (nu != nv) - (long long) (ou != ov[j]));
+            else c = (long long) w[j] * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov[j]));
+            acc += (xv[j] & MOVED) ? c : 2 * c;
+        }
+    }
+    if (inval) {
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+            if (v[j] != SENTINEL) a.dest_cache[v[j]] = NULL_PART;
+    }
+    return acc;
+}
+
+template<bool NC = true, int B = 4>
 __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 nthreads,
                                                  bool inval) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
@@ -719,35 +752,39 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
     const u32 nu = x & ~MOVED;
     const u32 ou = um ? ldj<NC>(&a.dest_part[u]) : nu;
     long long acc = 0;
-    for (u32 t0 = from + tid; t0 < to; t0 += 4 * nthreads) {
-        u32 v[4], xv[4], ov[4];
-        s32 w[4];
+    for (u32 t0 = from + tid; t0 < to; t0 += B * nthreads) {
+        u32 v[B];
+        s32 w[B];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < B; ++j) {
             const u32 t = t0 + j * nthreads;
             v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
             w[j] = t < to ? g_ew(a.g, beg + t) : 0;
         }
-        if (um) {
+        acc += delta_batch<B, NC>(a, nu, ou, um, v, w, inval);
+    }
+    return acc;
+}
+
+// The same over len entries staged in shared memory (one warp, B per lane).
+template<int B>
+__device__ __forceinline__ long long delta_staged(const JArgs &a, u32 u, const u32 *sadj, const s32 *sew, u32 len,
+                                                  bool inval) {
+    const u32 x = __ldg(&a.map[u]);
+    const bool um = (x & MOVED) != 0;
+    const u32 nu = x & ~MOVED;
+    const u32 ou = um ? __ldg(&a.dest_part[u]) : nu;
+    long long acc = 0;
+    for (u32 t0 = (u32) lane_id(); t0 < len; t0 += 32u * B) {
+        u32 v[B];
+        s32 w[B];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) xv[j] = v[j] != SENTINEL ? ldj<NC>(&a.map[v[j]]) : 0;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) ov[j] = (xv[j] & MOVED) ? ldj<NC>(&a.dest_part[v[j]]) : (xv[j] & ~MOVED);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (v[j] == SENTINEL) continue;
-                const u32 nv = xv[j] & ~MOVED;
-                long long c;
-                if (!a.code) c = (long long) w[j] * ((long long) (nu != nv) - (long long) (ou != ov[j]));
-                else c = (long long) w[j] * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov[j]));
-                acc += (xv[j] & MOVED) ? c : 2 * c;
-            }
+        for (int j = 0; j < B; ++j) {
+            const u32 t = t0 + 32u * j;
+            v[j] = t < len ? sadj[t] : SENTINEL;
+            w[j] = t < len ? (sew ? sew[t] : 1) : 0;
         }
-        if (inval) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (v[j] != SENTINEL) a.dest_cache[v[j]] = NULL_PART;
-        }
+        acc += delta_batch<B, true>(a, nu, ou, um, v, w, inval);
     }
     return acc;
 }
@@ -834,7 +871,8 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
 // gathers, so resident warps matter more than registers. The objective delta
 // is added with one atomic per warp, so no warp waits for the others of its
 // block at the end.
-__global__ void __launch_bounds__(BLOCK, 6) k_delta_chunk(JArgs a) {
+template<int B>
+__global__ void __launch_bounds__(BLOCK, B > 4 ? 4 : 6) k_delta_chunk(JArgs a) {
     u32 total = a.st->cnt[ST_HEAVY];
     if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
@@ -843,8 +881,34 @@ __global__ void __launch_bounds__(BLOCK, 6) k_delta_chunk(JArgs a) {
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         u32 u, from, to, nch;
         chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
-        acc += delta_range(a, u, from, to, lane_id(), 32, inval);
+        acc += delta_range<true, B>(a, u, from, to, lane_id(), 32, inval);
     }
+    acc = warp_sum<long long>(acc);
+    if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
+}
+
+// Chunk items of the delta pass with their row segments staged in shared
+// memory by bulk copies (stage.cuh), eight entries per lane in flight.
+constexpr int STAGE_BLOCK = 128;
+constexpr int STAGE_BLOCKS_PER_SM = 6;
+constexpr size_t stage_smem() { return (STAGE_BLOCK / 32) * sizeof(WarpStage); }
+
+__global__ void __launch_bounds__(STAGE_BLOCK, STAGE_BLOCKS_PER_SM) k_delta_staged(JArgs a) {
+    extern __shared__ __align__(16) unsigned char stage_sm[];
+    WarpStage &S = reinterpret_cast<WarpStage *>(stage_sm)[warp_in_block()];
+    u32 total = a.st->cnt[ST_HEAVY];
+    if (total > a.items_cap) total = a.items_cap;
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    const bool inval = scattered_inval(a);
+    long long acc = 0;
+    staged_items(
+        a.g, S, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps, total, &a.st->err,
+        [&](u32 i, u32 &u, u32 &from, u32 &to) {
+            u32 nch;
+            chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
+        },
+        [&](u32 u, const u32 *sadj, const s32 *sew, u32 len, u32) { acc += delta_staged<8>(a, u, sadj, sew, len, inval); },
+        [&](u32, u32) {});
     acc = warp_sum<long long>(acc);
     if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
 }
@@ -2014,6 +2078,9 @@ void set_big_smem() {
                                  (int) (34 * JW_SLOTS * sizeof(s32))));
     HP_CUDA(cudaFuncSetAttribute(k_jet_loop<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int) (34 * JW_SLOTS * sizeof(s32))));
+    // staged chunk kernels: the full shared-memory carveout, so that
+    // STAGE_BLOCKS_PER_SM blocks of stage_smem() bytes fit on an SM
+    HP_CUDA(cudaFuncSetAttribute(k_delta_staged, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     done.push_back(dev);
 }
 
@@ -2423,7 +2490,16 @@ void JetLevel::perform() {
         }
         {
             KernTimer kt1(c, "k_delta_chunk");
-            k_delta_chunk<<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+            if (c.tune.jet_chunk_mode == 2 && stage_ok(g)) {
+                const u32 blocks = (u32) std::min<u64>(((u64) items_cap * 32 + STAGE_BLOCK - 1) / STAGE_BLOCK,
+                                                       (u64) c.sm_count * STAGE_BLOCKS_PER_SM);
+                k_delta_staged<<<std::max<u32>(blocks, 1), STAGE_BLOCK, stage_smem(), c.stream>>>(a);
+            } else if (c.tune.jet_chunk_mode == 1) {
+                k_delta_chunk<8><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+            } else {
+                k_delta_chunk<4><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+            }
+            note_launch();
         }
         k_inval_unmark<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     }

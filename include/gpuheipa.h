@@ -217,7 +217,10 @@ int hp_coop_slot_release(int device);
  * many vertices, entries and entries per vertex; 0 = never), "jet_coop_rows"
  * (vertices per block of that grid),
  * "jet_hub_deg" (Jet connectivity passes with k <= 256: rows longer than this
- * are split into chunks of this many entries, one warp each; 64..4096).
+ * are split into chunks of this many entries, one warp each; 64..4096),
+ * "jet_chunk_mode" (the Jet chunk kernels read row entries 4 (0) or 8 (1) per
+ * lane from global memory, or (2) stage row segments in shared memory with
+ * bulk copies, 8 per lane; values above 2 are rejected).
  * Unknown names return HP_ERR_ARG. No counterpart in the reference. */
 int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
 

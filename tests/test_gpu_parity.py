@@ -339,6 +339,33 @@ def test_direct_launch_paths_equal(ctx):
         c2.close()
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+def test_chunk_modes_equal_oracle(mode):
+    # The chunk kernels of the per-kernel Jet path with eight entries per
+    # lane (1) or with bulk-copy staged row segments (2), on weighted and
+    # unit-weight graphs with hub rows, and on the mapping objective.
+    cases = [(H.Graph.rmat(15, 16, 0.57, 0.19, 0.19, 1, 10, 3), 64), (H.Graph.rmat(14, 16, seed=3), 32)]
+    m = H.Graph.rgg3d(20000, 14.0, 1, 100, seed=8, explicit_vw=True)
+    c = H.Context(0, 2 << 30)
+    try:
+        for name in ("jet_fused_max_n", "jet_coop_max_n"):
+            c.tune(name, 0)
+        c.tune("jet_chunk_mode", mode)
+        for g, k in cases:
+            part, cut = c.partition(g, k, 0.03, "default", 7)
+            opart, ocut = O.partition(to_oracle(g), k, 0.03, False, 7)
+            assert cut == ocut
+            np.testing.assert_array_equal(part, opart)
+        mp, J = c.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, "IM", 3)
+        want_m, want_j = O.map_im(to_oracle(m), [2, 4, 3], [1, 10, 100], 0.03, 3)
+        assert J == want_j
+        np.testing.assert_array_equal(mp, want_m)
+        with pytest.raises(H.HeiPaError):
+            c.tune("jet_chunk_mode", 3)
+    finally:
+        c.close()
+
+
 def test_arena_exhaustion_is_an_error():
     small = H.Context(0, 64 << 20)
     try:
