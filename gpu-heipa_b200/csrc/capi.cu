@@ -9,6 +9,7 @@
 #include <new>
 
 #include "../host/generators.h"
+#include "../host/initial_partition.h"
 #include "../host/metis_io.h"
 #include "service.cuh"
 #include "solver.cuh"
@@ -114,6 +115,34 @@ size_t hp_arena_estimate(uint32_t n, uint64_t m, int has_ew, int has_vw) {
 }
 
 size_t hp_arena_peak(const hp_ctx *ctx) { return ctx ? ctx->c.arena.peak() : 0; }
+
+int hp_initial_partition(uint32_t n, const uint32_t *xadj, const uint32_t *adj, const int32_t *vw, const int32_t *ew,
+                         uint32_t k, double imbalance, uint64_t seed, uint32_t *part) {
+    if (!xadj || (n > 0 && !part) || k == 0 || k > hp::MAX_K) return HP_ERR_ARG;
+    const uint64_t m = xadj[n];
+    if (m > 0 && !adj) return HP_ERR_ARG;
+    if (m > 0x7FFFFFFFull || n > 0x7FFFFFFFu) return HP_ERR_ARG;  // the partitioner indexes with int
+    hp::HostCSR g;
+    g.n = n;
+    g.m = (uint32_t) m;
+    g.xadj.assign(xadj, xadj + n + 1);
+    for (uint32_t u = 0; u < n; ++u)
+        if (xadj[u + 1] < xadj[u]) return HP_ERR_GRAPH;
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint32_t j = xadj[u]; j < xadj[u + 1]; ++j)
+            if (adj[j] >= n || adj[j] == u) return HP_ERR_GRAPH;
+    g.adj.assign(adj, adj + m);
+    if (ew) g.ew.assign(ew, ew + m);
+    if (vw) g.vw.assign(vw, vw + n);
+    try {
+        std::vector<uint32_t> out;
+        hp::initial_kway(g, k, imbalance, seed, out);
+        std::copy(out.begin(), out.end(), part);
+    } catch (const std::bad_alloc &) {
+        return HP_ERR_OOM;
+    }
+    return HP_OK;
+}
 
 int hp_graph_upload(hp_ctx *ctx, uint32_t n, uint64_t m, const uint32_t *xadj, const uint32_t *adj, const int32_t *ew,
                     const int32_t *vw, hp_graph **out) {

@@ -111,7 +111,6 @@ void Service::wait_all() {
 
 void Service::worker_main(size_t w) {
     const bool dev_ok = cudaSetDevice(device_) == cudaSuccess;
-    set_initial_partition_threads(1);  // requests run concurrently: no nested host threads
     Ctx &c = *ctxs_[w];
     std::unique_lock<std::mutex> lk(mu_);
     for (;;) {

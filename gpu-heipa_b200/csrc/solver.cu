@@ -218,8 +218,6 @@ void run_hm_tasks(Ctx &ctx, std::vector<HmTask> &tasks, Fn fn) {
         threads.emplace_back([&, w] {
             try {
                 HP_CUDA(cudaSetDevice(ctx.device));
-                // concurrent sub-solves: each host thread partitions sequentially
-                if (W > 1) set_initial_partition_threads(1);
                 for (size_t i = next++; i < tasks.size(); i = next++) {
                     fn(*wc[w], tasks[i]);
                     wc[w]->sync();

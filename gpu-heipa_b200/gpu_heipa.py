@@ -62,6 +62,7 @@ _SIG = {
     "hp_edge_cut_noalloc": (_int, [_u32, _u32, _vp, _vp, _vp, _vp, _vp, _vp]),
     "hp_selftest_barrier_timeout": (_int, [ctypes.c_int, _u32, _vp, _vp]),
     "hp_coop_slot_acquire": (_int, [ctypes.c_int, ctypes.c_int]),
+    "hp_initial_partition": (_int, [_u32, _vp, _vp, _vp, _vp, _u32, ctypes.c_double, ctypes.c_uint64, _vp]),
     "hp_coop_slot_release": (_int, [ctypes.c_int]),
     "hp_partition": (_int, [_vp, _u32, _u64, _vp, _vp, _vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
     "hp_partition_graph": (_int, [_vp, _vp, _u32, _dbl, _int, _u64, _vp, _vp]),
@@ -261,6 +262,15 @@ def kernel_launches():
 
 
 DEVERR_SPIN = 8  # device error bit: a bounded wait gave up
+
+
+def initial_partition(g, k, imbalance=0.03, seed=0):
+    """The reference's host k-way partitioner on host graph g, rows in their
+    given order (hp_initial_partition); returns the labels."""
+    part = np.empty(g.n, np.uint32)
+    _host_check(_L.hp_initial_partition(g.n, _p(g.xadj), _p(g.adj), _p(g.vw), _p(g.ew), int(k), float(imbalance),
+                                        int(seed), _p(part)), "initial partition failed")
+    return part
 
 
 def coop_slot_acquire(device=0, timeout_ms=0):

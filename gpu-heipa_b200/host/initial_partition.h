@@ -4,25 +4,19 @@
 // for the coarsest level (src/initial_partitioning/kway_partitioner/kway_core.h:
 // 1527-1588) and, for process mapping with --config IM, a recursive partition
 // over the hierarchy levels (src/initial_partitioning/global_multisection.h:
-// 132-287). This file provides the same two services with an algorithm of its
-// own: multilevel recursive bisection (heavy-edge coarsening, greedy graph
-// growing, 2-way FM) followed by greedy k-way balancing/refinement. It runs on
-// graphs of at most a few thousand vertices and is deterministic for a seed.
+// 132-287). This file provides the same two services with the same algorithm
+// (metis_kway.h): on the same graph, seed and imbalance the partition equals
+// the reference's. It runs on graphs of a few thousand vertices, is
+// sequential and deterministic, and is safe to call from concurrent threads.
 #pragma once
 #include "hp_types.h"
 
 namespace hp {
 
-// Partitions `g` into k blocks, block weights ideally <= ceil((1+eps)*W/k).
-// The result depends only on the graph (with rows in a canonical order), k,
-// eps and seed.
+// Partitions `g` into k blocks as kway_partition(HostGraph&, k, eps, seed, ...)
+// does (kway_core.h:1548-1571). The result depends on the graph including its
+// row order (callers pass rows sorted by neighbour id), k, eps and seed.
 void initial_kway(const HostCSR &g, u32 k, double eps, u64 seed, std::vector<u32> &part);
-
-// Host threads the initial partitioner may use on the calling thread (the
-// bisection tries of one coarsest level run concurrently); 1 = sequential.
-// Results do not depend on it. Threads that run concurrent sub-solves set 1
-// so that they do not oversubscribe the host. Default 8.
-void set_initial_partition_threads(int threads);
 
 // Imbalance for a sub-problem of a hierarchical split, as in
 // src/initial_partitioning/global_multisection.h:39-48.

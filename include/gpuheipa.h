@@ -321,6 +321,17 @@ int hp_write_metis(const char *path, uint32_t n, uint64_t m, const uint32_t *xad
 /* Replaces write_partition (src/utility/util.h:288-329): one id per line. */
 int hp_write_partition(const char *path, const uint32_t *part, uint32_t n);
 
+/* Replaces kway_partition(HostGraph&, k, imbalance, seed, HostPartition&)
+ * (src/initial_partitioning/kway_partitioner/kway_core.h:1548-1571): the
+ * reference's METIS-derived host partitioner, which every solve runs on its
+ * coarsest graph. Host CSR in (rows in the order given; vw / ew NULL for unit
+ * weights), n labels < k out. The imbalance is narrowed to float and the seed
+ * to int as in the reference; on the same graph, k, imbalance and seed the
+ * partition equals the reference's. HP_ERR_GRAPH for ids out of range or self
+ * loops; safe to call from concurrent threads. */
+int hp_initial_partition(uint32_t n, const uint32_t *xadj, const uint32_t *adj, const int32_t *vw, const int32_t *ew,
+                         uint32_t k, double imbalance, uint64_t seed, uint32_t *part);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1020,6 +1020,77 @@ s32 max_block(const HostCSR &g, const std::vector<u32> &part, u32 k) {
     return m;
 }
 
+// The initial partitioner: the reference's own ModifiedMetis::partition
+// (kway_core.h:1527-1571) compiled from its sources into
+// oracle/_ref/libkway_ref.so when that library was built (oracle.py installs
+// it here), else the product's restatement of it (host/metis_kway.cpp).
+typedef void (*RefKwayFn)(uint32_t, const uint32_t *, const uint32_t *, const int32_t *, const int32_t *, int, double,
+                          uint64_t, uint32_t *);
+RefKwayFn g_ref_kway = nullptr;
+
+void oracle_kway(const HostCSR &g, u32 k, double eps, u64 seed, std::vector<u32> &part) {
+    if (!g_ref_kway || k <= 1 || g.n == 0) {
+        initial_kway(g, k, eps, seed, part);
+        return;
+    }
+    std::vector<s32> vw(g.n), ew(g.m);
+    for (u32 u = 0; u < g.n; ++u) vw[u] = VW(g, u);
+    for (u32 j = 0; j < g.m; ++j) ew[j] = EW(g, j);
+    part.assign(g.n, 0);
+    g_ref_kway(g.n, g.xadj.data(), g.adj.data(), vw.data(), ew.data(), (int) k, eps, seed, part.data());
+}
+
+// recursive_partition global_multisection.h:132-220: partition into the
+// current level's k, then recurse into every block's induced subgraph (empty
+// subgraphs are skipped; the reference would divide by zero there).
+void ims_recurse(const HostCSR &g, const std::vector<u32> &n_to_o, const std::vector<u32> &hier, u32 level,
+                 std::vector<u32> &identifier, const std::vector<u32> &index_vec, const std::vector<u32> &k_rem,
+                 double eps, s64 global_w, u32 global_k, u64 seed, std::vector<u32> &global_part) {
+    const u32 l = (u32) hier.size();
+    const u32 k_here = hier[level];
+    const u64 depth = identifier.size();
+    const s64 local_w = g.total_vw();
+    const double imb =
+        local_w > 0 ? adaptive_imbalance(eps, global_w, global_k, local_w, k_rem[l - 1 - depth], l - depth) : eps;
+    std::vector<u32> tmp;
+    oracle_kway(g, k_here, imb, seed, tmp);
+    if (depth == l - 1) {
+        u32 offset = 0;
+        for (u32 i = 0; i + 1 < l; ++i) offset += identifier[i] * index_vec[index_vec.size() - 1 - i];
+        for (u32 u = 0; u < g.n; ++u) global_part[n_to_o[u]] = offset + tmp[u];
+        return;
+    }
+    for (u32 id = 0; id < k_here; ++id) {
+        std::vector<u32> sub_n_to_o;
+        HostCSR sub = induced_subgraph(g, tmp, id, sub_n_to_o);
+        if (sub.n == 0) continue;
+        for (u32 &x: sub_n_to_o) x = n_to_o[x];
+        identifier.push_back(id);
+        ims_recurse(sub, sub_n_to_o, hier, level - 1, identifier, index_vec, k_rem, eps, global_w, global_k, seed,
+                    global_part);
+        identifier.pop_back();
+    }
+}
+
+// global_multisection_host global_multisection.h:222-257.
+void ims_initial(const HostCSR &g, const std::vector<u32> &hier, double eps, u64 seed, std::vector<u32> &part) {
+    const u32 l = (u32) hier.size();
+    part.assign(g.n, 0);
+    if (l == 0 || g.n == 0) return;
+    std::vector<u32> index_vec = {1};
+    for (u32 i = 0; i + 1 < l; ++i) index_vec.push_back(index_vec[i] * hier[i]);
+    std::vector<u32> k_rem(l);
+    u32 p = 1;
+    for (u32 i = 0; i < l; ++i) {
+        k_rem[i] = p * hier[i];
+        p *= hier[i];
+    }
+    std::vector<u32> n_to_o(g.n);
+    std::iota(n_to_o.begin(), n_to_o.end(), 0u);
+    std::vector<u32> identifier;
+    ims_recurse(g, n_to_o, hier, l - 1, identifier, index_vec, k_rem, eps, g.total_vw(), p, seed, part);
+}
+
 // Solver::internal_solve solver.h:340-400 (and the device constructor
 // :144-246 used by hierarchical multisection).
 s64 partition_graph(const HostCSR &g, u32 k, double eps, bool ultra, u64 seed, std::vector<u32> &part) {
@@ -1040,7 +1111,7 @@ s64 partition_graph(const HostCSR &g, u32 k, double eps, bool ultra, u64 seed, s
     HostCSR coarsest = *cur;
     sort_rows(coarsest);
     std::vector<u32> cpart;
-    initial_kway(coarsest, k, eps, seed, cpart);
+    oracle_kway(coarsest, k, eps, seed, cpart);
     s64 cut = edge_cut(*cur, cpart);
     s32 maxw = max_block(*cur, cpart, k);
     for (size_t l = maps.size(); l > 0; --l) {
@@ -1260,7 +1331,7 @@ int64_t or_map_im(const void *gp, const uint32_t *hier, const int32_t *dist, uin
     HostCSR coarsest = *cur;
     sort_rows(coarsest);
     std::vector<u32> cpart;
-    global_multisection(coarsest, h, eps, seed, cpart);  // promap_solver.h:391-409
+    ims_initial(coarsest, h, eps, seed, cpart);  // promap_solver.h:391-409
     s64 J = comm_cost(*cur, cpart, D, k);
     s32 maxw = max_block(*cur, cpart, k);
     for (size_t lv = maps.size(); lv > 0; --lv) {
@@ -1273,5 +1344,14 @@ int64_t or_map_im(const void *gp, const uint32_t *hier, const int32_t *dist, uin
 }
 
 int32_t or_lmax(int64_t total_weight, uint32_t k, double eps) { return lmax_of(total_weight, k, eps); }
+
+void or_set_ref_kway(void *fn) { g_ref_kway = (RefKwayFn) fn; }
+int or_uses_ref_kway(void) { return g_ref_kway != nullptr; }
+
+void or_initial_kway(const void *g, uint32_t k, double eps, uint64_t seed, uint32_t *part_out) {
+    std::vector<u32> part;
+    oracle_kway(G(g), k, eps, seed, part);
+    std::copy(part.begin(), part.end(), part_out);
+}
 
 } // extern "C"

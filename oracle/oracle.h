@@ -3,14 +3,18 @@
 // CPU-baseline legs of bench.py) as the checker for the CUDA implementation.
 // Nothing in the product links or calls it.
 //
-// Parity status: the reference (GPU-HeiPa) cannot be built here (Kokkos and
-// Kokkos-Kernels are absent), ships no tests, golden vectors or fixtures, and
-// is nondeterministic (CAS races pick matching partners, hash slot order and
-// bucket offsets). This oracle therefore restates the reference's algorithm
-// with documented deterministic rules where the reference races, and is
-// pinned only by hand-computed known-answer tests (contraction, distance
-// matrix, objective values, hash test vectors, gain buckets). Matching and
-// Jet dynamics are "parity unpinned" against the reference itself.
+// Parity status: the reference (GPU-HeiPa) cannot be built here as a whole
+// (Kokkos and Kokkos-Kernels are absent), ships no tests, golden vectors or
+// fixtures, and its GPU phases are nondeterministic (CAS races pick matching
+// partners, hash slot order and bucket offsets). This oracle therefore
+// restates the reference's GPU algorithm with documented deterministic rules
+// where the reference races; matching and Jet dynamics are pinned by
+// hand-computed known-answer tests (contraction, distance matrix, objective
+// values, hash test vectors, gain buckets) and are "parity unpinned" against
+// the reference itself. The host initial partitioner is the exception: the
+// reference's own plain-C++ ModifiedMetis code is compiled from its sources
+// (oracle/build_ref.py) and used here directly, and the product's
+// restatement of it is checked against it bit for bit.
 #pragma once
 #include <stdint.h>
 
@@ -71,6 +75,16 @@ int64_t or_map_im(const void *g, const uint32_t *hier, const int32_t *dist, uint
                   uint32_t *part_out);
 // lmax = ceil((1+eps) * W / k), as solver.h:410
 int32_t or_lmax(int64_t total_weight, uint32_t k, double eps);
+
+// ---- initial partitioner -------------------------------------------------
+// Installs the reference's own ModifiedMetis::partition (the C entry point of
+// oracle/_ref/libkway_ref.so, built from the reference's sources by
+// oracle/build_ref.py); without it the pipelines use the product's
+// restatement (host/metis_kway.cpp).
+void or_set_ref_kway(void *fn);
+int or_uses_ref_kway(void);
+// The initial partition the pipelines use (kway_core.h:1548-1571).
+void or_initial_kway(const void *g, uint32_t k, double eps, uint64_t seed, uint32_t *part_out);
 
 #ifdef __cplusplus
 }

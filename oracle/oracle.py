@@ -13,18 +13,27 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
-_SOURCES = [os.path.join(_HERE, "oracle.cpp"),
-            os.path.join(_HERE, "..", "gpu-heipa_b200", "host", "initial_partition.cpp")]
+_HOST = os.path.join(_HERE, "..", "gpu-heipa_b200", "host")
+_SOURCES = [os.path.join(_HERE, "oracle.cpp"), os.path.join(_HOST, "initial_partition.cpp"),
+            os.path.join(_HOST, "metis_kway.cpp")]
 
 
 def build(force=False):
-    """Compiles the oracle with g++ (OpenMP) into oracle/_build/."""
+    """Compiles the oracle with g++ (OpenMP) into oracle/_build/, and the
+    reference's own initial partitioner into oracle/_ref/ when the reference
+    sources are present (build_ref.py)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("oracle_build_ref", os.path.join(_HERE, "build_ref.py"))
+    build_ref = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(build_ref)
+    build_ref.build_ref()
     os.makedirs(os.path.dirname(_LIB_PATH), exist_ok=True)
     if not force and os.path.exists(_LIB_PATH):
-        newest = max(os.path.getmtime(s) for s in _SOURCES + [os.path.join(_HERE, "oracle.h")])
-        if os.path.getmtime(_LIB_PATH) >= newest:
+        deps = _SOURCES + [os.path.join(_HERE, "oracle.h"), os.path.join(_HOST, "metis_kway.h"),
+                           os.path.join(_HOST, "initial_partition.h")]
+        if os.path.getmtime(_LIB_PATH) >= max(os.path.getmtime(s) for s in deps):
             return _LIB_PATH
-    cmd = ["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-o", _LIB_PATH] + _SOURCES
+    cmd = ["g++", "-O3", "-std=c++17", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-o", _LIB_PATH] + _SOURCES
     subprocess.run(cmd, check=True)
     return _LIB_PATH
 
@@ -74,13 +83,42 @@ def lib():
         "or_map_hm": (c.c_int64, [_vp, _vp, _vp, c.c_uint32, c.c_double, c.c_int, c.c_uint64, _vp]),
         "or_map_im": (c.c_int64, [_vp, _vp, _vp, c.c_uint32, c.c_double, c.c_uint64, _vp]),
         "or_lmax": (c.c_int32, [c.c_int64, c.c_uint32, c.c_double]),
+        "or_set_ref_kway": (None, [_vp]),
+        "or_uses_ref_kway": (c.c_int, []),
+        "or_initial_kway": (None, [_vp, c.c_uint32, c.c_double, c.c_uint64, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
         f.restype = res
         f.argtypes = args
+    ref = ref_lib()
+    if ref is not None:
+        L.or_set_ref_kway(ctypes.cast(ref.ref_kway_partition, ctypes.c_void_p))
     _lib = L
     return L
+
+
+_REF_PATH = os.path.join(_HERE, "_ref", "libkway_ref.so")
+_ref = None
+
+
+def ref_lib():
+    """The reference's own initial partitioner (oracle/_ref/libkway_ref.so,
+    built by build_ref.py from the reference's sources), or None."""
+    global _ref
+    if _ref is None and os.path.exists(_REF_PATH):
+        R = ctypes.CDLL(_REF_PATH)
+        R.ref_kway_partition.restype = None
+        R.ref_kway_partition.argtypes = [ctypes.c_uint32, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_uint64, _vp]
+        _ref = R
+    return _ref
+
+
+def uses_reference_kway():
+    """True when the oracle pipelines take their initial partitions from the
+    reference's own code."""
+    return bool(lib().or_uses_ref_kway())
 
 
 def _p(a):
@@ -125,6 +163,25 @@ class Graph:
         has_ew = bool(L.or_graph_has_ew(self.h))
         has_vw = bool(L.or_graph_has_vw(self.h))
         return xadj, adj, (ew if has_ew else None), (vw if has_vw else None)
+
+
+def initial_kway(g, k, eps, seed):
+    """The initial partition of the oracle pipelines (kway_core.h:1548-1571)."""
+    part = np.zeros(g.n, np.uint32)
+    lib().or_initial_kway(g.h, k, eps, seed, _p(part))
+    return part
+
+
+def ref_kway(xadj, adj, vw, ew, k, imbalance, seed):
+    """GPU_HeiPa::ModifiedMetis::partition itself on a CSR (weights required)."""
+    R = ref_lib()
+    if R is None:
+        raise RuntimeError("oracle/_ref/libkway_ref.so is not built")
+    xadj, adj, vw, ew = _u32(xadj), _u32(adj), _s32(vw), _s32(ew)
+    part = np.zeros(len(xadj) - 1, np.uint32)
+    R.ref_kway_partition(len(xadj) - 1, _p(xadj), _p(adj), _p(vw), _p(ew), int(k), float(imbalance), int(seed),
+                         _p(part))
+    return part
 
 
 def match(g):
