@@ -138,6 +138,7 @@ struct Tunables {
     u32 jet_coop_rows = 1024;          // vertices per block of that grid
     u32 jet_hub_deg = 1024;            // Jet table passes: rows above this length are cut into chunks of it (64..4096)
     u32 jet_chunk_mode = 0;            // chunk kernels: 0 = 4 entries per lane, 1 = 8, 2 = bulk-copy staged rows
+    u32 jet_hub_conn = 1;              // per-kernel Jet loop: keep hub-row connectivity up to date (1) or rescan (0)
 };
 
 struct Ctx {

@@ -35,6 +35,10 @@ constexpr u32 NOKEY = 0xFFFFFFFFu;
 // bit marks the vertices that changed block in this iteration; their old
 // label is in dest_part[] (the reference's swap, perform_moves :794-795).
 constexpr u32 MOVED = 0x80000000u;
+constexpr u32 DL_LABEL = 0xFFu;      // dlab: label (k <= HUB_K = 256)
+constexpr u32 DL_MOVED = 0x100u;     // dlab: changed block in this perform
+constexpr u32 DL_SLOT_SHIFT = 9;     // dlab: hub slot + 1 above this bit
+constexpr u32 DL_MAX_HUBS = (1u << (32 - DL_SLOT_SHIFT)) - 2;
 
 // Block-tier table size: a row never has more distinct blocks than k.
 inline u32 block_slots_for(u32 k) {
@@ -69,6 +73,12 @@ struct JArgs {
     u32 *hubcnt;  // hub rows: finished chunks per row slot (zero between uses)
     u32 hub_cap;  // row slots of hubacc / hubcnt
     u32 hub_deg;  // hub threshold and chunk length (entries) when hubacc is set
+    // Tracked hub connectivity (per-kernel level loop, k <= HUB_K): hubacc
+    // then holds, for every hub row, its connection to each block, kept up to
+    // date by the delta pass, and dlab[v] packs v's label (DL_LABEL bits), its
+    // moved bit (DL_MOVED) and its hub slot + 1 (above DL_SLOT_SHIFT, 0 = not
+    // a hub). Null when hub rows are rescanned in chunks on every pass.
+    u32 *dlab;
     s32 *abacc;  // afterburner partial sums of multi-chunk rows (zero between uses)
     u32 *abcnt;  // afterburner finished chunks of multi-chunk rows (zero between uses)
     DevStatus *st;
@@ -509,7 +519,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
-        if (a.hubacc) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
+        if (a.hubacc && !a.dlab) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
     }
     block_count(&a.st->cnt[ST_AUX], (unsigned long long *) &a.st->sum[4], nrec, erec);
 }
@@ -719,7 +729,31 @@ template<int B, bool NC>
 __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou, bool um, const u32 (&v)[B],
                                                  const s32 (&w)[B], bool inval) {
     long long acc = 0;
-    if (um) {
+    if (um && a.dlab) {
+        // tracked hubs: one gather of dlab gives the neighbour's label, moved
+        // bit and hub slot; hub neighbours move w from ou to nu in their
+        // connectivity (integer atomics: the result does not depend on order)
+        u32 xv[B], ov[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) xv[j] = v[j] != SENTINEL ? ldj<NC>(&a.dlab[v[j]]) : 0;
+#pragma unroll
+        for (int j = 0; j < B; ++j) ov[j] = (xv[j] & DL_MOVED) ? ldj<NC>(&a.dest_part[v[j]]) : (xv[j] & DL_LABEL);
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            if (v[j] == SENTINEL) continue;
+            const u32 nv = xv[j] & DL_LABEL;
+            long long c;
+            if (!a.code) c = (long long) w[j] * ((long long) (nu != nv) - (long long) (ou != ov[j]));
+            else c = (long long) w[j] * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov[j]));
+            acc += (xv[j] & DL_MOVED) ? c : 2 * c;
+            const u32 hs = xv[j] >> DL_SLOT_SHIFT;
+            if (hs) {
+                s32 *conn = a.hubacc + (u64) (hs - 1) * a.k;
+                atomicSub(&conn[ou], w[j]);
+                atomicAdd(&conn[nu], w[j]);
+            }
+        }
+    } else if (um) {
         u32 xv[B], ov[B];
 #pragma unroll
         for (int j = 0; j < B; ++j) xv[j] = v[j] != SENTINEL ? ldj<NC>(&a.map[v[j]]) : 0;
@@ -808,6 +842,7 @@ __global__ void k_inval_unmark(JArgs a) {
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const u32 u = a.moves[i];
         a.map[u] &= ~MOVED;
+        if (a.dlab) a.dlab[u] &= ~DL_MOVED;
     }
 }
 
@@ -939,6 +974,7 @@ __global__ void __launch_bounds__(BLOCK) k_apply(JArgs a) {
             }
         }
         a.map[u] = ou != nu ? (nu | MOVED) : nu;
+        if (a.dlab) a.dlab[u] = (a.dlab[u] & ~(DL_LABEL | DL_MOVED)) | nu | (ou != nu ? DL_MOVED : 0u);
         a.dest_part[u] = ou;
         a.dest_cache[u] = NULL_PART;
         entries += a.g.rowlen[u];
@@ -1109,7 +1145,7 @@ __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
-        if (a.hubacc) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
+        if (a.hubacc && !a.dlab) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
     }
 }
 
@@ -1197,6 +1233,77 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub(JArgs a, u32 ratio, RbArgs r) 
         __syncwarp();
         if (KIND == 0) lp_finish_group<false, true>(a, u, ratio, T, nullptr, nullptr);
         else rb_finish_group<KIND == 2, false, true>(a, r, u, T, nullptr, nullptr);
+    }
+}
+
+// Tracked hubs: one warp per hub row of the pass's hub list (heavy2) loads
+// the row's connectivity from hubacc into its direct table and completes the
+// row with the ordinary finishing code (gain: KIND 0, weak: 1, strong: 2).
+template<int KIND>
+__global__ void __launch_bounds__(JW_BLOCK) k_hub_tracked(JArgs a, u32 ratio, RbArgs r) {
+    u32 *w = warp_table<true>(a.k);
+    s32 *tv = (s32 *) w;
+    const ConnTable<false, true> T{w, tv, 0, a.k};
+    const u32 total = a.st->cnt[ST_HEAVY2];
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const u32 u = a.heavy2[i];
+        const u32 hs = a.dlab[u] >> DL_SLOT_SHIFT;
+        if (hs == 0 || hs > a.hub_cap) {  // not a tracked hub: cannot happen for rows above hub_deg
+            if (lane_id() == 0) set_error(&a.st->err, DEV_ERR_RANGE);
+            continue;
+        }
+        const s32 *conn = a.hubacc + (u64) (hs - 1) * a.k;
+        for (u32 b = lane_id(); b < a.k; b += 32) tv[b] = conn[b];
+        __syncwarp();
+        if (KIND == 0) lp_finish_group<false, true>(a, u, ratio, T, nullptr, nullptr);
+        else rb_finish_group<KIND == 2, false, true>(a, r, u, T, nullptr, nullptr);
+    }
+}
+
+// Level set-up of tracked hubs: numbers the hub rows (rows of more than
+// hub_deg entries) and writes dlab for every vertex; emits the chunk items of
+// the hub rows for k_hub_build.
+__global__ void __launch_bounds__(BLOCK) k_hub_number(JArgs a) {
+    const u64 stride = (u64) gridDim.x * blockDim.x;
+    for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
+        const u32 u = (u32) (base + threadIdx.x);
+        const bool hub = u < a.g.n && a.g.rowlen[u] > a.hub_deg;
+        const u32 slot = warp_append(&a.st->cnt[ST_HEAVY2], hub);
+        const bool ok = hub && slot < a.hub_cap && slot < DL_MAX_HUBS;
+        if (hub && !ok) set_error(&a.st->err, DEV_ERR_RANGE);
+        if (ok) a.heavy2[slot] = u;
+        if (u < a.g.n) a.dlab[u] = a.map[u] | (ok ? (slot + 1) << DL_SLOT_SHIFT : 0u);
+        emit_hub_chunks(a, slot, ok ? a.g.rowlen[u] : 0u);
+    }
+}
+
+// Builds the tracked connectivity of every hub row from its chunks: each warp
+// adds its chunk's block sums to the row's hubacc entries.
+__global__ void __launch_bounds__(JW_BLOCK) k_hub_build(JArgs a) {
+    u32 *w = warp_table<true>(a.k);
+    s32 *tv = (s32 *) w;
+    u32 total = a.st->cnt[ST_CHUNKS];
+    if (total > a.items_cap) total = a.items_cap;
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    const u32 lane = lane_id();
+    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+        const unsigned long long it = a.items[i];
+        const u32 h = (u32) (it >> 32);
+        const u32 u = a.heavy2[h];
+        const u32 len = __ldg(&a.g.rowlen[u]);
+        const u32 from = (u32) it * a.hub_deg;
+        const u32 to = len - from < a.hub_deg ? len : from + a.hub_deg;
+        dtable_build_range<false>(a, u, tv, from, to);
+        s32 *acc = a.hubacc + (u64) h * a.k;
+        for (u32 b = lane; b < a.k; b += 32) {
+            const s32 v = tv[b];
+            if (v) {
+                atomicAdd(&acc[b], v);
+                tv[b] = 0;
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -2043,6 +2150,7 @@ JArgs make_args(JetLevel &L) {
     a.hubcnt = L.hubcnt;
     a.hub_cap = L.hub_cap;
     a.hub_deg = L.hub_deg;
+    a.dlab = L.dlab;
     a.abcnt = L.abcnt;
     a.st = L.ctx->d_status;
     a.blk_slots = L.blk_slots;
@@ -2197,6 +2305,7 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     hubacc = nullptr;
     hubcnt = nullptr;
     hub_cap = 0;
+    dlab = nullptr;
     if (warp_direct && k <= HUB_K) {
         hub_cap = (u32) std::min<u64>(n, g.m / hub_deg + 1);
         hubacc = c.balloc<s32>((u64) hub_cap * k);
@@ -2216,6 +2325,21 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     HP_CUDA(cudaMemsetAsync(gain1, 0, sizeof(s32) * n, c.stream));
     block_weights(c, g, map, k, bw);
     set_big_smem();
+}
+
+void JetLevel::track_hubs() {
+    if (!hubacc || !ctx->tune.jet_hub_conn || hub_cap > DL_MAX_HUBS) return;
+    Ctx &c = *ctx;
+    ProfScope prof(c, "jet.track_hubs");
+    dlab = c.balloc<u32>(g.n);
+    c.zero_counters();
+    JArgs a = make_args(*this);
+    k_hub_number<<<c.grid(g.n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    k_hub_build<<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(a);
+    note_launch();
+    HP_LAUNCH_CHECK();
+    c.check_device_error();
+    c.zero_counters();
 }
 
 void JetLevel::gain_pass(u32 ratio_pct) {
@@ -2239,7 +2363,10 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     }
     {
         KernTimer kt(c, "k_lp_block");
-        if (hubacc) {
+        if (dlab) {
+            k_hub_tracked<0><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
+                               c.stream>>>(a, ratio_pct, RbArgs{});
+        } else if (hubacc) {
             k_hub<0><<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(
                 a, ratio_pct, RbArgs{});
         } else {
@@ -2308,7 +2435,10 @@ void JetLevel::weak() {
         }
         {
             KernTimer kt1(c, "k_weak_block");
-            if (hubacc) {
+            if (dlab) {
+                k_hub_tracked<1><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
+                                   c.stream>>>(a, 0u, r);
+            } else if (hubacc) {
                 k_hub<1><<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                c.stream>>>(a, 0u, r);
             } else {
@@ -2393,7 +2523,10 @@ void JetLevel::strong() {
         }
         {
             KernTimer kt1(c, "k_strong_block");
-            if (hubacc) {
+            if (dlab) {
+                k_hub_tracked<2><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
+                                   c.stream>>>(a, 0u, r);
+            } else if (hubacc) {
                 k_hub<2><<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                c.stream>>>(a, 0u, r);
             } else {
@@ -2694,6 +2827,7 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
             }
         }
     }
+    L.track_hubs();
     for (u32 ratio: ratios) {
         u32 balance_iteration = 0, iteration = 0;
         while (iteration < JET_MAX_ITERATIONS) {

@@ -67,6 +67,7 @@ struct JetLevel {
     s32 *hubacc = nullptr;  // hub-row connectivity accumulators (direct tables, small k), or null
     u32 *hubcnt = nullptr;  // hub-row finished-chunk counters
     u32 hub_cap = 0;        // hub-row slots
+    u32 *dlab = nullptr;    // tracked hubs: packed label / moved bit / hub slot per vertex (null: untracked)
     u32 hub_deg = 0;        // hub threshold and chunk length (entries)
     s32 *abacc = nullptr;  // afterburner partial sums of multi-chunk rows
     u32 *abcnt = nullptr;  // afterburner finished-chunk counts of multi-chunk rows
@@ -91,6 +92,11 @@ struct JetLevel {
     void perform();
     // Single pass helpers used by tests: recompute gains for all vertices
     // whose cache is invalid (the "Jet-gain" kernel).
+    // Per-kernel level loop with direct tables and k <= 256: builds the
+    // connectivity of every hub row once (Tunables::jet_hub_conn), after
+    // which the delta pass keeps it up to date and the gain and rebalance
+    // passes read it instead of rescanning hub rows.
+    void track_hubs();
     void gain_pass(u32 ratio_pct);
 
     // One Jet iteration: the step (0 = lp with ratio_pct, 1 = weak, 2 =

@@ -220,7 +220,9 @@ int hp_coop_slot_release(int device);
  * are split into chunks of this many entries, one warp each; 64..4096),
  * "jet_chunk_mode" (the Jet chunk kernels read row entries 4 (0) or 8 (1) per
  * lane from global memory, or (2) stage row segments in shared memory with
- * bulk copies, 8 per lane; values above 2 are rejected).
+ * bulk copies, 8 per lane; values above 2 are rejected), "jet_hub_conn" (1:
+ * the per-kernel Jet loop keeps the block connectivity of hub rows up to date
+ * from the moved vertices instead of rescanning the rows every pass; 0: rescan).
  * Unknown names return HP_ERR_ARG. No counterpart in the reference. */
 int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
 
