@@ -74,11 +74,22 @@ struct JArgs {
     u32 hub_cap;  // row slots of hubacc / hubcnt
     u32 hub_deg;  // hub threshold and chunk length (entries) when hubacc is set
     // Tracked hub connectivity (per-kernel level loop, k <= HUB_K): hubacc
-    // then holds, for every hub row, its connection to each block, kept up to
-    // date by the delta pass, and dlab[v] packs v's label (DL_LABEL bits), its
-    // moved bit (DL_MOVED) and its hub slot + 1 (above DL_SLOT_SHIFT, 0 = not
-    // a hub). Null when hub rows are rescanned in chunks on every pass.
+    // then holds, for every hub row h and block b, the row's connection to b
+    // at hubacc[b * hub_cap + h] (block-major, so that the counters of one
+    // busy hub lie on k different cache lines), kept up to date by the delta
+    // pass; dlab[v] packs v's label (DL_LABEL bits), its moved bit (DL_MOVED)
+    // and its hub slot + 1 (above DL_SLOT_SHIFT, 0 = not a hub). Null when hub
+    // rows are rescanned in chunks on every pass.
     u32 *dlab;
+    // A perform whose moved rows hold more than hub_track_max entries does
+    // not update the hub sums but sets *hub_stale; the next pass that reads
+    // them first rebuilds them from the hub rows (hub_items: chunk items of
+    // all hub rows, hub_vertex: the row of each hub slot).
+    unsigned long long hub_track_max;
+    u32 *hub_stale;
+    const unsigned long long *hub_items;
+    u32 hub_nitems;
+    const u32 *hub_vertex;
     s32 *abacc;  // afterburner partial sums of multi-chunk rows (zero between uses)
     u32 *abcnt;  // afterburner finished chunks of multi-chunk rows (zero between uses)
     DevStatus *st;
@@ -510,8 +521,10 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
             } else {
                 const u32 len = a.g.rowlen[u];
                 ++nrec;
-                erec += len;
                 cls = table_tier(len, a.k, a.hubacc ? a.hub_deg : JW_DEG);
+                // a tracked hub row is not scanned: it reads its k sums
+                // (counted as k / 3 entries of 12 bytes)
+                erec += (cls == 2 && a.dlab) ? (a.k + 2) / 3 : len;
                 if (cls == 0) lp_thread(a, u, ratio);
             }
         }
@@ -725,9 +738,15 @@ __global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
 // marks an empty slot) of a row whose vertex has new label nu and old label
 // ou (um: it changed block). All B labels are gathered, then the old labels
 // of moved neighbours, so B dependent gathers are in flight at a time.
+// Whether this perform updates the tracked hub sums (else it marks them
+// stale): read by every delta kernel after k_apply has counted the entries.
+__device__ __forceinline__ bool hub_update_now(const JArgs &a) {
+    return a.dlab && (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] <= a.hub_track_max;
+}
+
 template<int B, bool NC>
 __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou, bool um, const u32 (&v)[B],
-                                                 const s32 (&w)[B], bool inval) {
+                                                 const s32 (&w)[B], bool inval, bool hub_upd) {
     long long acc = 0;
     if (um && a.dlab) {
         // tracked hubs: one gather of dlab gives the neighbour's label, moved
@@ -747,10 +766,9 @@ __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou,
             else c = (long long) w[j] * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov[j]));
             acc += (xv[j] & DL_MOVED) ? c : 2 * c;
             const u32 hs = xv[j] >> DL_SLOT_SHIFT;
-            if (hs) {
-                s32 *conn = a.hubacc + (u64) (hs - 1) * a.k;
-                atomicSub(&conn[ou], w[j]);
-                atomicAdd(&conn[nu], w[j]);
+            if (hs && hub_upd) {
+                atomicSub(&a.hubacc[(u64) ou * a.hub_cap + (hs - 1)], w[j]);
+                atomicAdd(&a.hubacc[(u64) nu * a.hub_cap + (hs - 1)], w[j]);
             }
         }
     } else if (um) {
@@ -779,7 +797,7 @@ __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou,
 
 template<bool NC = true, int B = 4>
 __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 nthreads,
-                                                 bool inval) {
+                                                 bool inval, bool hub_upd = false) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     const u32 x = ldj<NC>(&a.map[u]);
     const bool um = (x & MOVED) != 0;
@@ -795,7 +813,7 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
             v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
             w[j] = t < to ? g_ew(a.g, beg + t) : 0;
         }
-        acc += delta_batch<B, NC>(a, nu, ou, um, v, w, inval);
+        acc += delta_batch<B, NC>(a, nu, ou, um, v, w, inval, hub_upd);
     }
     return acc;
 }
@@ -803,7 +821,7 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
 // The same over len entries staged in shared memory (one warp, B per lane).
 template<int B>
 __device__ __forceinline__ long long delta_staged(const JArgs &a, u32 u, const u32 *sadj, const s32 *sew, u32 len,
-                                                  bool inval) {
+                                                  bool inval, bool hub_upd) {
     const u32 x = __ldg(&a.map[u]);
     const bool um = (x & MOVED) != 0;
     const u32 nu = x & ~MOVED;
@@ -818,7 +836,7 @@ __device__ __forceinline__ long long delta_staged(const JArgs &a, u32 u, const u
             v[j] = t < len ? sadj[t] : SENTINEL;
             w[j] = t < len ? (sew ? sew[t] : 1) : 0;
         }
-        acc += delta_batch<B, true>(a, nu, ou, um, v, w, inval);
+        acc += delta_batch<B, true>(a, nu, ou, um, v, w, inval, hub_upd);
     }
     return acc;
 }
@@ -872,6 +890,8 @@ __device__ __forceinline__ void block_add_s64(long long v, long long *dst) {
 __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
     const bool inval = scattered_inval(a);
+    const bool hub_upd = hub_update_now(a);
+    if (a.dlab && !hub_upd && blockIdx.x == 0 && threadIdx.x == 0) *a.hub_stale = 1u;
     const u64 stride = (u64) gridDim.x * blockDim.x;
     long long acc = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -880,7 +900,7 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
         if (i < total) {
             u = a.moves[i];
             const u32 len = __ldg(&a.g.rowlen[u]);
-            if (len <= CHUNK_THREAD_MAX) acc += delta_range(a, u, 0, len, 0, 1, inval);
+            if (len <= CHUNK_THREAD_MAX) acc += delta_range(a, u, 0, len, 0, 1, inval, hub_upd);
             else nch = chunks_of(len);
         }
         warp_emit_chunks(a, u, nch, &a.st->cnt[ST_HEAVY]);
@@ -912,11 +932,12 @@ __global__ void __launch_bounds__(BLOCK, B > 4 ? 4 : 6) k_delta_chunk(JArgs a) {
     if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     const bool inval = scattered_inval(a);
+    const bool hub_upd = hub_update_now(a);
     long long acc = 0;
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         u32 u, from, to, nch;
         chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
-        acc += delta_range<true, B>(a, u, from, to, lane_id(), 32, inval);
+        acc += delta_range<true, B>(a, u, from, to, lane_id(), 32, inval, hub_upd);
     }
     acc = warp_sum<long long>(acc);
     if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
@@ -935,6 +956,7 @@ __global__ void __launch_bounds__(STAGE_BLOCK, STAGE_BLOCKS_PER_SM) k_delta_stag
     if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     const bool inval = scattered_inval(a);
+    const bool hub_upd = hub_update_now(a);
     long long acc = 0;
     staged_items(
         a.g, S, (blockIdx.x * blockDim.x + threadIdx.x) >> 5, warps, total, &a.st->err,
@@ -942,7 +964,7 @@ __global__ void __launch_bounds__(STAGE_BLOCK, STAGE_BLOCKS_PER_SM) k_delta_stag
             u32 nch;
             chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
         },
-        [&](u32 u, const u32 *sadj, const s32 *sew, u32 len, u32) { acc += delta_staged<8>(a, u, sadj, sew, len, inval); },
+        [&](u32 u, const u32 *sadj, const s32 *sew, u32 len, u32) { acc += delta_staged<8>(a, u, sadj, sew, len, inval, hub_upd); },
         [&](u32, u32) {});
     acc = warp_sum<long long>(acc);
     if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
@@ -1246,6 +1268,7 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_tracked(JArgs a, u32 ratio, Rb
     const ConnTable<false, true> T{w, tv, 0, a.k};
     const u32 total = a.st->cnt[ST_HEAVY2];
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *a.hub_stale = 0u;  // the rebuild (if any) has finished
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const u32 u = a.heavy2[i];
         const u32 hs = a.dlab[u] >> DL_SLOT_SHIFT;
@@ -1253,8 +1276,7 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_tracked(JArgs a, u32 ratio, Rb
             if (lane_id() == 0) set_error(&a.st->err, DEV_ERR_RANGE);
             continue;
         }
-        const s32 *conn = a.hubacc + (u64) (hs - 1) * a.k;
-        for (u32 b = lane_id(); b < a.k; b += 32) tv[b] = conn[b];
+        for (u32 b = lane_id(); b < a.k; b += 32) tv[b] = a.hubacc[(u64) b * a.hub_cap + (hs - 1)];
         __syncwarp();
         if (KIND == 0) lp_finish_group<false, true>(a, u, ratio, T, nullptr, nullptr);
         else rb_finish_group<KIND == 2, false, true>(a, r, u, T, nullptr, nullptr);
@@ -1273,38 +1295,49 @@ __global__ void __launch_bounds__(BLOCK) k_hub_number(JArgs a) {
         const bool ok = hub && slot < a.hub_cap && slot < DL_MAX_HUBS;
         if (hub && !ok) set_error(&a.st->err, DEV_ERR_RANGE);
         if (ok) a.heavy2[slot] = u;
+        if (ok) const_cast<u32 *>(a.hub_vertex)[slot] = u;
         if (u < a.g.n) a.dlab[u] = a.map[u] | (ok ? (slot + 1) << DL_SLOT_SHIFT : 0u);
         emit_hub_chunks(a, slot, ok ? a.g.rowlen[u] : 0u);
     }
 }
 
-// Builds the tracked connectivity of every hub row from its chunks: each warp
-// adds its chunk's block sums to the row's hubacc entries.
-__global__ void __launch_bounds__(JW_BLOCK) k_hub_build(JArgs a) {
+// Builds the tracked connectivity of every hub row from the chunk items of
+// all hub rows (a.hub_items); each warp adds its chunk's block sums to the
+// row's hubacc entries. With `only_if_stale`, does nothing unless the sums
+// were marked stale.
+__global__ void __launch_bounds__(JW_BLOCK) k_hub_build(JArgs a, int only_if_stale) {
+    if (only_if_stale && *(volatile u32 *) a.hub_stale == 0u) return;
     u32 *w = warp_table<true>(a.k);
     s32 *tv = (s32 *) w;
-    u32 total = a.st->cnt[ST_CHUNKS];
-    if (total > a.items_cap) total = a.items_cap;
+    const u32 total = a.hub_nitems;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     const u32 lane = lane_id();
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
-        const unsigned long long it = a.items[i];
+        const unsigned long long it = a.hub_items[i];
         const u32 h = (u32) (it >> 32);
-        const u32 u = a.heavy2[h];
+        const u32 u = a.hub_vertex[h];
         const u32 len = __ldg(&a.g.rowlen[u]);
         const u32 from = (u32) it * a.hub_deg;
         const u32 to = len - from < a.hub_deg ? len : from + a.hub_deg;
         dtable_build_range<false>(a, u, tv, from, to);
-        s32 *acc = a.hubacc + (u64) h * a.k;
         for (u32 b = lane; b < a.k; b += 32) {
             const s32 v = tv[b];
             if (v) {
-                atomicAdd(&acc[b], v);
+                atomicAdd(&a.hubacc[(u64) b * a.hub_cap + h], v);
                 tv[b] = 0;
             }
         }
         __syncwarp();
     }
+}
+
+// Zeroes the tracked hub sums when they were marked stale (first half of a
+// rebuild; k_hub_build(a, 1) follows).
+__global__ void k_hub_zero(JArgs a) {
+    if (*(volatile u32 *) a.hub_stale == 0u) return;
+    const u64 total = (u64) a.hub_cap * a.k;
+    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (u64) gridDim.x * blockDim.x)
+        a.hubacc[i] = 0;
 }
 
 // underloaded_blocks (:614-627): ordered list of blocks below max_b_w.
@@ -2151,6 +2184,11 @@ JArgs make_args(JetLevel &L) {
     a.hub_cap = L.hub_cap;
     a.hub_deg = L.hub_deg;
     a.dlab = L.dlab;
+    a.hub_track_max = L.hub_track_max;
+    a.hub_stale = L.hub_stale;
+    a.hub_items = L.hub_items;
+    a.hub_nitems = L.hub_nitems;
+    a.hub_vertex = L.hub_vertex;
     a.abcnt = L.abcnt;
     a.st = L.ctx->d_status;
     a.blk_slots = L.blk_slots;
@@ -2306,6 +2344,11 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     hubcnt = nullptr;
     hub_cap = 0;
     dlab = nullptr;
+    hub_stale = nullptr;
+    hub_items = nullptr;
+    hub_nitems = 0;
+    hub_vertex = nullptr;
+    hub_track_max = 0;
     if (warp_direct && k <= HUB_K) {
         hub_cap = (u32) std::min<u64>(n, g.m / hub_deg + 1);
         hubacc = c.balloc<s32>((u64) hub_cap * k);
@@ -2332,14 +2375,43 @@ void JetLevel::track_hubs() {
     Ctx &c = *ctx;
     ProfScope prof(c, "jet.track_hubs");
     dlab = c.balloc<u32>(g.n);
+    hub_stale = c.balloc<u32>(1);
+    u32 *vertex = c.balloc<u32>(hub_cap);
+    hub_vertex = vertex;
+    HP_CUDA(cudaMemsetAsync(hub_stale, 0, sizeof(u32), c.stream));
     c.zero_counters();
     JArgs a = make_args(*this);
     k_hub_number<<<c.grid(g.n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    k_hub_build<<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(a);
+    HP_LAUNCH_CHECK();
+    // keep the hub rows' chunk items (the items array is reused by every pass)
+    const DevStatus &st = c.read_status();
+    if (st.err) throw HpError{HP_ERR_DEVICE, "hub numbering reported error bits " + std::to_string(st.err)};
+    hub_nitems = std::min<u32>(st.cnt[ST_CHUNKS], items_cap);
+    unsigned long long *its = c.balloc<unsigned long long>(hub_nitems);
+    HP_CUDA(cudaMemcpyAsync(its, items, sizeof(unsigned long long) * hub_nitems, cudaMemcpyDeviceToDevice, c.stream));
+    hub_items = its;
+    // sums of all hub rows' lengths: updates pay while the moved rows hold at
+    // most jet_hub_track_pct percent of that many entries
+    const unsigned long long hub_entries = (unsigned long long) hub_nitems * hub_deg;
+    hub_track_max = hub_entries / 100 * c.tune.jet_hub_track_pct;
+    a = make_args(*this);
+    k_hub_build<<<c.grid((u64) hub_nitems * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(
+        a, 0);
     note_launch();
     HP_LAUNCH_CHECK();
-    c.check_device_error();
     c.zero_counters();
+}
+
+// Rebuilds the tracked hub sums if the last perform marked them stale
+// (device-side check; no host synchronisation).
+void JetLevel::refresh_hubs() {
+    if (!dlab) return;
+    Ctx &c = *ctx;
+    JArgs a = make_args(*this);
+    k_hub_zero<<<c.grid((u64) hub_cap * k, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+    k_hub_build<<<c.grid((u64) hub_nitems * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(
+        a, 1);
+    note_launch();
 }
 
 void JetLevel::gain_pass(u32 ratio_pct) {
@@ -2348,6 +2420,7 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     JArgs a = make_args(*this);
     const u32 n = g.n;
     gain_rec = c.instr.begin(c.stream, "jet_gain", 0.0);
+    refresh_hubs();
     {
         KernTimer kt(c, "k_lp_dispatch");
         k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
@@ -2417,6 +2490,7 @@ void JetLevel::weak() {
     k_under<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, under, &c.d_status->cnt[ST_AUX]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, under, keys};
+    refresh_hubs();
     {
         ProfScope p2(c, "weak.pick");
         KernTimer kt(c, "k_weak_pick");
@@ -2505,6 +2579,7 @@ void JetLevel::strong() {
     k_maxv<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, &c.d_status->imax[1]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, nullptr, keys};
+    refresh_hubs();
     {
         ProfScope p2(c, "strong.pick");
         KernTimer kt(c, "k_strong_pick");

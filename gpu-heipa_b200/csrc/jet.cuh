@@ -68,6 +68,11 @@ struct JetLevel {
     u32 *hubcnt = nullptr;  // hub-row finished-chunk counters
     u32 hub_cap = 0;        // hub-row slots
     u32 *dlab = nullptr;    // tracked hubs: packed label / moved bit / hub slot per vertex (null: untracked)
+    u32 *hub_stale = nullptr;                         // tracked hubs: sums to be rebuilt before the next pass
+    const unsigned long long *hub_items = nullptr;    // tracked hubs: chunk items of all hub rows
+    u32 hub_nitems = 0;
+    const u32 *hub_vertex = nullptr;                  // tracked hubs: row of each hub slot
+    unsigned long long hub_track_max = 0;             // tracked hubs: update while moved entries <= this
     u32 hub_deg = 0;        // hub threshold and chunk length (entries)
     s32 *abacc = nullptr;  // afterburner partial sums of multi-chunk rows
     u32 *abcnt = nullptr;  // afterburner finished-chunk counts of multi-chunk rows
@@ -97,6 +102,7 @@ struct JetLevel {
     // which the delta pass keeps it up to date and the gain and rebalance
     // passes read it instead of rescanning hub rows.
     void track_hubs();
+    void refresh_hubs();
     void gain_pass(u32 ratio_pct);
 
     // One Jet iteration: the step (0 = lp with ratio_pct, 1 = weak, 2 =

@@ -222,7 +222,10 @@ int hp_coop_slot_release(int device);
  * lane from global memory, or (2) stage row segments in shared memory with
  * bulk copies, 8 per lane; values above 2 are rejected), "jet_hub_conn" (1:
  * the per-kernel Jet loop keeps the block connectivity of hub rows up to date
- * from the moved vertices instead of rescanning the rows every pass; 0: rescan).
+ * from the moved vertices instead of rescanning the rows every pass; 0: rescan),
+ * "jet_hub_track_pct" (with jet_hub_conn = 1: a perform whose moved rows hold
+ * more entries than this percentage of all hub-row entries lets the next pass
+ * rebuild the hub sums from the rows instead of updating them).
  * Unknown names return HP_ERR_ARG. No counterpart in the reference. */
 int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
 
