@@ -75,11 +75,11 @@ struct JArgs {
     u32 hub_deg;  // hub threshold and chunk length (entries) when hubacc is set
     // Tracked hub connectivity (per-kernel level loop, k <= HUB_K): hubacc
     // then holds, for every hub row h and block b, the row's connection to b
-    // at hubacc[b * hub_cap + h] (block-major, so that the counters of one
-    // busy hub lie on k different cache lines), kept up to date by the delta
-    // pass; dlab[v] packs v's label (DL_LABEL bits), its moved bit (DL_MOVED)
-    // and its hub slot + 1 (above DL_SLOT_SHIFT, 0 = not a hub). Null when hub
-    // rows are rescanned in chunks on every pass.
+    // at hubacc[h * k + b] (the two counters one moved neighbour changes share
+    // a cache line; a block-major layout measured slower), kept up to date by
+    // the delta pass; dlab[v] packs v's label (DL_LABEL bits), its moved bit
+    // (DL_MOVED) and its hub slot + 1 (above DL_SLOT_SHIFT, 0 = not a hub).
+    // Null when hub rows are rescanned in chunks on every pass.
     u32 *dlab;
     // A perform whose moved rows hold more than hub_track_max entries does
     // not update the hub sums but sets *hub_stale; the next pass that reads
@@ -767,8 +767,8 @@ __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou,
             acc += (xv[j] & DL_MOVED) ? c : 2 * c;
             const u32 hs = xv[j] >> DL_SLOT_SHIFT;
             if (hs && hub_upd) {
-                atomicSub(&a.hubacc[(u64) ou * a.hub_cap + (hs - 1)], w[j]);
-                atomicAdd(&a.hubacc[(u64) nu * a.hub_cap + (hs - 1)], w[j]);
+                atomicSub(&a.hubacc[(u64) (hs - 1) * a.k + ou], w[j]);
+                atomicAdd(&a.hubacc[(u64) (hs - 1) * a.k + nu], w[j]);
             }
         }
     } else if (um) {
@@ -1276,7 +1276,7 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_tracked(JArgs a, u32 ratio, Rb
             if (lane_id() == 0) set_error(&a.st->err, DEV_ERR_RANGE);
             continue;
         }
-        for (u32 b = lane_id(); b < a.k; b += 32) tv[b] = a.hubacc[(u64) b * a.hub_cap + (hs - 1)];
+        for (u32 b = lane_id(); b < a.k; b += 32) tv[b] = a.hubacc[(u64) (hs - 1) * a.k + b];
         __syncwarp();
         if (KIND == 0) lp_finish_group<false, true>(a, u, ratio, T, nullptr, nullptr);
         else rb_finish_group<KIND == 2, false, true>(a, r, u, T, nullptr, nullptr);
@@ -1323,7 +1323,7 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_build(JArgs a, int only_if_sta
         for (u32 b = lane; b < a.k; b += 32) {
             const s32 v = tv[b];
             if (v) {
-                atomicAdd(&a.hubacc[(u64) b * a.hub_cap + h], v);
+                atomicAdd(&a.hubacc[(u64) h * a.k + b], v);
                 tv[b] = 0;
             }
         }
