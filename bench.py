@@ -570,6 +570,49 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def run_quality(args, world, rank, local):
+    """Quality over seeds 1..N (north star check (d)): the objective of every
+    seed on the GPU and, with --quality-oracle, of the CPU oracle restatement
+    on the same graph and seed, with the geometric means."""
+    if rank != 0:
+        return 0
+    import gpu_heipa as H
+    wl = WORKLOADS[args.workload]
+    g = make_graph(H, wl, args.seed)
+    scale = 2 if wl["task"] == "map" else 1
+    seeds = list(range(1, args.quality_seeds + 1))
+    gpu, cpu, times = [], [], []
+    with H.Context(local, scale * H.arena_estimate(g.n, g.m, g.ew is not None, g.vw is not None)) as ctx:
+        dg = ctx.upload(g)
+        part = np.empty(g.n, np.uint32)
+        for sd in seeds:
+            a = argparse.Namespace(**vars(args))
+            a.seed = sd
+            t0 = time.perf_counter()
+            gpu.append(int(solve_device(ctx, dg, wl, a, part)))
+            times.append(time.perf_counter() - t0)
+        dg.free()
+    if args.quality_oracle:
+        O, og = oracle_graph(g)
+        for sd in seeds:
+            a = argparse.Namespace(**vars(args))
+            a.seed = sd
+            cpu.append(int(oracle_solve(O, og, wl, a)))
+
+    def geomean(xs):
+        return float(np.exp(np.mean(np.log(np.asarray(xs, np.float64))))) if xs and min(xs) > 0 else None
+
+    line = {"quality_seeds": len(seeds), "workload": wl["desc"], "config": config_of(wl, args),
+            "objective": "cut" if wl["task"] == "partition" else "J", "seeds": seeds, "gpu": gpu,
+            "gpu_geomean": geomean(gpu), "gpu_ms_median": 1000 * statistics.median(times)}
+    if cpu:
+        line.update({"cpu_oracle": cpu, "cpu_oracle_geomean": geomean(cpu),
+                     "gpu_over_cpu_geomean": (geomean(gpu) / geomean(cpu)) if geomean(cpu) else None,
+                     "identical_every_seed": gpu == cpu})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -583,6 +626,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--kernel-timers", action="store_true", help="print every kernel timer to stderr")
     ap.add_argument("--workers", type=int, default=8, help="concurrent requests (batch / served workloads)")
+    ap.add_argument("--quality-seeds", type=int, default=0,
+                    help="instead of timing: objective over seeds 1..N on the GPU (geometric mean)")
+    ap.add_argument("--quality-oracle", action="store_true", help="with --quality-seeds: also the CPU oracle")
     ap.add_argument("--tune", action="append", default=[], metavar="NAME=VALUE",
                     help="launch-structure threshold (hp_tune), e.g. jet_graph_max_m=0 for profiling runs")
     args = ap.parse_args()
@@ -593,7 +639,9 @@ def main():
         dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     try:
         task = WORKLOADS[args.workload]["task"]
-        if args.impl == "reference":
+        if args.quality_seeds > 0 and task not in ("batch", "served"):
+            rc = run_quality(args, world, rank, local)
+        elif args.impl == "reference":
             if task in ("batch", "served"):
                 print(json.dumps({"impl": "reference", "unavailable": "the batched and served workloads have no "
                                   "CPU restatement; their plain runs on the GPU are the comparison"}), flush=True)
