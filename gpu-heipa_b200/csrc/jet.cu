@@ -35,10 +35,15 @@ constexpr u32 NOKEY = 0xFFFFFFFFu;
 // bit marks the vertices that changed block in this iteration; their old
 // label is in dest_part[] (the reference's swap, perform_moves :794-795).
 constexpr u32 MOVED = 0x80000000u;
-constexpr u32 DL_LABEL = 0xFFu;      // dlab: label (k <= HUB_K = 256)
-constexpr u32 DL_MOVED = 0x100u;     // dlab: changed block in this perform
-constexpr u32 DL_SLOT_SHIFT = 9;     // dlab: hub slot + 1 above this bit
-constexpr u32 DL_MAX_HUBS = (1u << (32 - DL_SLOT_SHIFT)) - 2;
+// dlab (per-kernel level loop): label, moved bit, old label and hub slot of
+// a vertex in one word, so that the delta pass needs one gather per
+// neighbour.
+constexpr unsigned long long DL_LABEL = 0xFFFFull;           // label (k <= MAX_K)
+constexpr unsigned long long DL_MOVED = 1ull << 16;          // changed block in this perform
+constexpr int DL_OLD_SHIFT = 17;                              // old label (valid with DL_MOVED)
+constexpr unsigned long long DL_OLD = 0xFFFFull << DL_OLD_SHIFT;
+constexpr int DL_SLOT_SHIFT = 33;                             // tracked hub slot + 1 (0: not a tracked hub)
+constexpr u32 DL_MAX_HUBS = 0x7FFFFFFEu;
 
 // Block-tier table size: a row never has more distinct blocks than k.
 inline u32 block_slots_for(u32 k) {
@@ -73,14 +78,21 @@ struct JArgs {
     u32 *hubcnt;  // hub rows: finished chunks per row slot (zero between uses)
     u32 hub_cap;  // row slots of hubacc / hubcnt
     u32 hub_deg;  // hub threshold and chunk length (entries) when hubacc is set
-    // Tracked hub connectivity (per-kernel level loop, k <= HUB_K): hubacc
-    // then holds, for every hub row h and block b, the row's connection to b
-    // at hubacc[h * k + b] (the two counters one moved neighbour changes share
-    // a cache line; a block-major layout measured slower), kept up to date by
-    // the delta pass; dlab[v] packs v's label (DL_LABEL bits), its moved bit
-    // (DL_MOVED) and its hub slot + 1 (above DL_SLOT_SHIFT, 0 = not a hub).
-    // Null when hub rows are rescanned in chunks on every pass.
-    u32 *dlab;
+    // Per-kernel level loop: dlab[v] packs v's label (DL_LABEL bits), its
+    // moved bit (DL_MOVED), its old label while moved (DL_OLD) and, with
+    // tracked hubs, its hub slot + 1 (above DL_SLOT_SHIFT). Null in the
+    // single-launch level loop.
+    unsigned long long *dlab;
+    // Afterburner records (per-kernel level loop): gain1 (low 32 bits),
+    // dest_part (next 16) and label (top 16) of a vertex, written by the
+    // filter, so that a neighbour costs one gather. Null: separate arrays.
+    unsigned long long *abrec;
+    // Tracked hub connectivity (k <= HUB_K, hub_stale set): hubacc then
+    // holds, for every hub row h and block b, the row's connection to b at
+    // hubacc[h * k + b] (the two counters one moved neighbour changes share a
+    // cache line; a block-major layout measured slower), kept up to date by
+    // the delta pass. Without tracking, hub rows are rescanned in chunks on
+    // every pass.
     // A perform whose moved rows hold more than hub_track_max entries does
     // not update the hub sums but sets *hub_stale; the next pass that reads
     // them first rebuilds them from the hub rows (hub_items: chunk items of
@@ -524,7 +536,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
                 cls = table_tier(len, a.k, a.hubacc ? a.hub_deg : JW_DEG);
                 // a tracked hub row is not scanned: it reads its k sums
                 // (counted as k / 3 entries of 12 bytes)
-                erec += (cls == 2 && a.dlab) ? (a.k + 2) / 3 : len;
+                erec += (cls == 2 && a.hub_stale) ? (a.k + 2) / 3 : len;
                 if (cls == 0) lp_thread(a, u, ratio);
             }
         }
@@ -532,7 +544,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
-        if (a.hubacc && !a.dlab) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
+        if (a.hubacc && !a.hub_stale) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
     }
     block_count(&a.st->cnt[ST_AUX], (unsigned long long *) &a.st->sum[4], nrec, erec);
 }
@@ -598,13 +610,14 @@ __global__ void __launch_bounds__(BLOCK) k_lp_filter(JArgs a) {
         const u32 u = (u32) (base + threadIdx.x);
         bool c = false;
         if (u < a.g.n) {
-            c = a.dest_part[u] != NO_MOVE && a.lock[u] == 0;
-            if (c) {
-                a.gain1[u] = a.gain_cache[u];
-            } else {
-                a.gain1[u] = GAIN_MIN;
-                a.lock[u] = 0;
-            }
+            const u32 dp = a.dest_part[u];
+            c = dp != NO_MOVE && a.lock[u] == 0;
+            const s32 g1 = c ? a.gain_cache[u] : GAIN_MIN;
+            a.gain1[u] = g1;
+            if (!c) a.lock[u] = 0;
+            if (a.abrec)
+                a.abrec[u] = (unsigned long long) (u32) g1 | ((unsigned long long) (dp & 0xFFFFu) << 32) |
+                             ((unsigned long long) (a.map[u] & 0xFFFFu) << 48);
         }
         const u32 s = block_append(&a.st->cnt[ST_CAND], c, sm);
         if (c) a.cand[s] = u;
@@ -632,17 +645,29 @@ __device__ __forceinline__ s32 ab_range(const JArgs &a, u32 u, s32 ug, u32 ou, u
             w[j] = t < to ? g_ew(a.g, beg + t) : 0;
         }
         // only neighbours that move first (higher gain, or equal gain and a
-        // lower id) contribute: their target and label are gathered after
-        // the gains, still four at a time
+        // lower id) contribute: their target and label come with the gain in
+        // one record (abrec) or are gathered after the gains
         bool first[4];
+        if (a.abrec) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) vg[j] = v[j] != SENTINEL ? ldj<NC>(&a.gain1[v[j]]) : 0;
+            for (int j = 0; j < 4; ++j) {
+                const unsigned long long r = v[j] != SENTINEL ? ldj<NC>(&a.abrec[v[j]]) : 0ull;
+                vg[j] = (s32) (u32) r;
+                nv[j] = (u32) (r >> 32) & 0xFFFFu;
+                ov[j] = (u32) (r >> 48);
+            }
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
-            if (first[j]) {
-                nv[j] = ldj<NC>(&a.dest_part[v[j]]);
-                ov[j] = ldj<NC>(&a.map[v[j]]);
+            for (int j = 0; j < 4; ++j) first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) vg[j] = v[j] != SENTINEL ? ldj<NC>(&a.gain1[v[j]]) : 0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
+                if (first[j]) {
+                    nv[j] = ldj<NC>(&a.dest_part[v[j]]);
+                    ov[j] = ldj<NC>(&a.map[v[j]]);
+                }
             }
         }
 #pragma unroll
@@ -741,7 +766,7 @@ __global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
 // Whether this perform updates the tracked hub sums (else it marks them
 // stale): read by every delta kernel after k_apply has counted the entries.
 __device__ __forceinline__ bool hub_update_now(const JArgs &a) {
-    return a.dlab && (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] <= a.hub_track_max;
+    return a.hub_stale && (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] <= a.hub_track_max;
 }
 
 template<int B, bool NC>
@@ -749,23 +774,23 @@ __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou,
                                                  const s32 (&w)[B], bool inval, bool hub_upd) {
     long long acc = 0;
     if (um && a.dlab) {
-        // tracked hubs: one gather of dlab gives the neighbour's label, moved
-        // bit and hub slot; hub neighbours move w from ou to nu in their
-        // connectivity (integer atomics: the result does not depend on order)
-        u32 xv[B], ov[B];
+        // one gather of dlab gives the neighbour's label, moved bit, old
+        // label and hub slot; tracked hub neighbours move w from ou to nu in
+        // their connectivity (integer atomics: the sums do not depend on
+        // their order)
+        unsigned long long xv[B];
 #pragma unroll
-        for (int j = 0; j < B; ++j) xv[j] = v[j] != SENTINEL ? ldj<NC>(&a.dlab[v[j]]) : 0;
-#pragma unroll
-        for (int j = 0; j < B; ++j) ov[j] = (xv[j] & DL_MOVED) ? ldj<NC>(&a.dest_part[v[j]]) : (xv[j] & DL_LABEL);
+        for (int j = 0; j < B; ++j) xv[j] = v[j] != SENTINEL ? ldj<NC>(&a.dlab[v[j]]) : 0ull;
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             if (v[j] == SENTINEL) continue;
-            const u32 nv = xv[j] & DL_LABEL;
+            const u32 nv = (u32) (xv[j] & DL_LABEL);
+            const u32 ov = (xv[j] & DL_MOVED) ? (u32) ((xv[j] & DL_OLD) >> DL_OLD_SHIFT) : nv;
             long long c;
-            if (!a.code) c = (long long) w[j] * ((long long) (nu != nv) - (long long) (ou != ov[j]));
-            else c = (long long) w[j] * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov[j]));
+            if (!a.code) c = (long long) w[j] * ((long long) (nu != nv) - (long long) (ou != ov));
+            else c = (long long) w[j] * ((long long) D(a, nu, nv) - (long long) D(a, ou, ov));
             acc += (xv[j] & DL_MOVED) ? c : 2 * c;
-            const u32 hs = xv[j] >> DL_SLOT_SHIFT;
+            const u32 hs = (u32) (xv[j] >> DL_SLOT_SHIFT);
             if (hs && hub_upd) {
                 atomicSub(&a.hubacc[(u64) (hs - 1) * a.k + ou], w[j]);
                 atomicAdd(&a.hubacc[(u64) (hs - 1) * a.k + nu], w[j]);
@@ -891,7 +916,7 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
     const bool inval = scattered_inval(a);
     const bool hub_upd = hub_update_now(a);
-    if (a.dlab && !hub_upd && blockIdx.x == 0 && threadIdx.x == 0) *a.hub_stale = 1u;
+    if (a.hub_stale && !hub_upd && blockIdx.x == 0 && threadIdx.x == 0) *a.hub_stale = 1u;
     const u64 stride = (u64) gridDim.x * blockDim.x;
     long long acc = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -996,7 +1021,9 @@ __global__ void __launch_bounds__(BLOCK) k_apply(JArgs a) {
             }
         }
         a.map[u] = ou != nu ? (nu | MOVED) : nu;
-        if (a.dlab) a.dlab[u] = (a.dlab[u] & ~(DL_LABEL | DL_MOVED)) | nu | (ou != nu ? DL_MOVED : 0u);
+        if (a.dlab)
+            a.dlab[u] = (a.dlab[u] & ~(DL_LABEL | DL_MOVED | DL_OLD)) | nu |
+                        (ou != nu ? DL_MOVED | ((unsigned long long) ou << DL_OLD_SHIFT) : 0ull);
         a.dest_part[u] = ou;
         a.dest_cache[u] = NULL_PART;
         entries += a.g.rowlen[u];
@@ -1167,7 +1194,7 @@ __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
-        if (a.hubacc && !a.dlab) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
+        if (a.hubacc && !a.hub_stale) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
     }
 }
 
@@ -1271,7 +1298,7 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_tracked(JArgs a, u32 ratio, Rb
     if (blockIdx.x == 0 && threadIdx.x == 0) *a.hub_stale = 0u;  // the rebuild (if any) has finished
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const u32 u = a.heavy2[i];
-        const u32 hs = a.dlab[u] >> DL_SLOT_SHIFT;
+        const u32 hs = (u32) (a.dlab[u] >> DL_SLOT_SHIFT);
         if (hs == 0 || hs > a.hub_cap) {  // not a tracked hub: cannot happen for rows above hub_deg
             if (lane_id() == 0) set_error(&a.st->err, DEV_ERR_RANGE);
             continue;
@@ -1296,7 +1323,7 @@ __global__ void __launch_bounds__(BLOCK) k_hub_number(JArgs a) {
         if (hub && !ok) set_error(&a.st->err, DEV_ERR_RANGE);
         if (ok) a.heavy2[slot] = u;
         if (ok) const_cast<u32 *>(a.hub_vertex)[slot] = u;
-        if (u < a.g.n) a.dlab[u] = a.map[u] | (ok ? (slot + 1) << DL_SLOT_SHIFT : 0u);
+        if (u < a.g.n) a.dlab[u] = a.map[u] | (ok ? (unsigned long long) (slot + 1) << DL_SLOT_SHIFT : 0ull);
         emit_hub_chunks(a, slot, ok ? a.g.rowlen[u] : 0u);
     }
 }
@@ -1329,6 +1356,11 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_build(JArgs a, int only_if_sta
         }
         __syncwarp();
     }
+}
+
+// dlab of every vertex without tracked hubs: the label alone.
+__global__ void k_dlab_init(JArgs a) {
+    for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < a.g.n; u += gridDim.x * blockDim.x) a.dlab[u] = a.map[u];
 }
 
 // Zeroes the tracked hub sums when they were marked stale (first half of a
@@ -2184,6 +2216,7 @@ JArgs make_args(JetLevel &L) {
     a.hub_cap = L.hub_cap;
     a.hub_deg = L.hub_deg;
     a.dlab = L.dlab;
+    a.abrec = L.abrec;
     a.hub_track_max = L.hub_track_max;
     a.hub_stale = L.hub_stale;
     a.hub_items = L.hub_items;
@@ -2344,6 +2377,7 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     hubcnt = nullptr;
     hub_cap = 0;
     dlab = nullptr;
+    abrec = nullptr;
     hub_stale = nullptr;
     hub_items = nullptr;
     hub_nitems = 0;
@@ -2370,11 +2404,17 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     set_big_smem();
 }
 
-void JetLevel::track_hubs() {
-    if (!hubacc || !ctx->tune.jet_hub_conn || hub_cap > DL_MAX_HUBS) return;
+void JetLevel::prepare_kernel_loop() {
     Ctx &c = *ctx;
-    ProfScope prof(c, "jet.track_hubs");
-    dlab = c.balloc<u32>(g.n);
+    ProfScope prof(c, "jet.prepare");
+    dlab = c.balloc<unsigned long long>(g.n);
+    abrec = c.balloc<unsigned long long>(g.n);
+    if (!hubacc || !c.tune.jet_hub_conn || hub_cap > DL_MAX_HUBS) {
+        JArgs a = make_args(*this);
+        k_dlab_init<<<c.grid(g.n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        HP_LAUNCH_CHECK();
+        return;
+    }
     hub_stale = c.balloc<u32>(1);
     u32 *vertex = c.balloc<u32>(hub_cap);
     hub_vertex = vertex;
@@ -2405,7 +2445,7 @@ void JetLevel::track_hubs() {
 // Rebuilds the tracked hub sums if the last perform marked them stale
 // (device-side check; no host synchronisation).
 void JetLevel::refresh_hubs() {
-    if (!dlab) return;
+    if (!hub_stale) return;
     Ctx &c = *ctx;
     JArgs a = make_args(*this);
     k_hub_zero<<<c.grid((u64) hub_cap * k, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
@@ -2436,7 +2476,7 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     }
     {
         KernTimer kt(c, "k_lp_block");
-        if (dlab) {
+        if (hub_stale) {
             k_hub_tracked<0><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                c.stream>>>(a, ratio_pct, RbArgs{});
         } else if (hubacc) {
@@ -2509,7 +2549,7 @@ void JetLevel::weak() {
         }
         {
             KernTimer kt1(c, "k_weak_block");
-            if (dlab) {
+            if (hub_stale) {
                 k_hub_tracked<1><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                    c.stream>>>(a, 0u, r);
             } else if (hubacc) {
@@ -2598,7 +2638,7 @@ void JetLevel::strong() {
         }
         {
             KernTimer kt1(c, "k_strong_block");
-            if (dlab) {
+            if (hub_stale) {
                 k_hub_tracked<2><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                    c.stream>>>(a, 0u, r);
             } else if (hubacc) {
@@ -2902,7 +2942,7 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
             }
         }
     }
-    L.track_hubs();
+    L.prepare_kernel_loop();
     for (u32 ratio: ratios) {
         u32 balance_iteration = 0, iteration = 0;
         while (iteration < JET_MAX_ITERATIONS) {

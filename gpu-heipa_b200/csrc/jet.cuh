@@ -67,7 +67,8 @@ struct JetLevel {
     s32 *hubacc = nullptr;  // hub-row connectivity accumulators (direct tables, small k), or null
     u32 *hubcnt = nullptr;  // hub-row finished-chunk counters
     u32 hub_cap = 0;        // hub-row slots
-    u32 *dlab = nullptr;    // tracked hubs: packed label / moved bit / hub slot per vertex (null: untracked)
+    unsigned long long *dlab = nullptr;   // per-kernel loop: packed label / moved / old label / hub slot
+    unsigned long long *abrec = nullptr;  // per-kernel loop: packed gain / target / label (afterburner)
     u32 *hub_stale = nullptr;                         // tracked hubs: sums to be rebuilt before the next pass
     const unsigned long long *hub_items = nullptr;    // tracked hubs: chunk items of all hub rows
     u32 hub_nitems = 0;
@@ -97,11 +98,12 @@ struct JetLevel {
     void perform();
     // Single pass helpers used by tests: recompute gains for all vertices
     // whose cache is invalid (the "Jet-gain" kernel).
-    // Per-kernel level loop with direct tables and k <= 256: builds the
-    // connectivity of every hub row once (Tunables::jet_hub_conn), after
-    // which the delta pass keeps it up to date and the gain and rebalance
-    // passes read it instead of rescanning hub rows.
-    void track_hubs();
+    // Before the per-kernel level loop: packed per-vertex words for the delta
+    // pass and the afterburner, and, with direct tables and k <= 256, the
+    // connectivity of every hub row (Tunables::jet_hub_conn), after which the
+    // delta pass keeps it up to date and the gain and rebalance passes read
+    // it instead of rescanning hub rows.
+    void prepare_kernel_loop();
     void refresh_hubs();
     void gain_pass(u32 ratio_pct);
 

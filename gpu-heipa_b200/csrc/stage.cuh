@@ -54,12 +54,7 @@ __device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void proxy_fence_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long *bar, u32 bytes) {
-    unsigned long long state;
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
-                 : "=l"(state)
-                 : "r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-    (void) state;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, u32 bytes, unsigned long long *bar) {
