@@ -219,29 +219,47 @@ void Ctx::destroy() {
 namespace {
 std::mutex g_coop_mu;
 std::condition_variable g_coop_cv;
-std::map<int, bool> g_coop_taken;  // device -> a cooperative grid holds the slot
+// device -> blocks of cooperative grids running; ALL_TAKEN while one caller
+// holds the whole budget
+std::map<int, unsigned long long> g_coop_used;
+constexpr unsigned long long ALL_TAKEN = ~0ull;
+inline u32 share_of(u32 blocks, u32 budget) {
+    if (budget == 0) budget = 1;
+    return blocks == 0 ? 1u : (blocks < budget ? blocks : budget);
+}
 }  // namespace
 
-void CoopSlots::acquire(int device) {
+void CoopSlots::acquire(int device, u32 blocks, u32 budget) {
+    const u32 t = share_of(blocks, budget);
     std::unique_lock<std::mutex> lock(g_coop_mu);
-    bool &taken = g_coop_taken[device];
-    g_coop_cv.wait(lock, [&] { return !taken; });
-    taken = true;
+    unsigned long long &used = g_coop_used[device];
+    g_coop_cv.wait(lock, [&] { return used != ALL_TAKEN && used + t <= (budget ? budget : 1u); });
+    used += t;
 }
 
-bool CoopSlots::try_acquire_for(int device, int timeout_ms) {
+void CoopSlots::release(int device, u32 blocks, u32 budget) {
+    const u32 t = share_of(blocks, budget);
+    {
+        std::lock_guard<std::mutex> lock(g_coop_mu);
+        unsigned long long &used = g_coop_used[device];
+        if (used != ALL_TAKEN) used = used >= t ? used - t : 0;
+    }
+    g_coop_cv.notify_all();
+}
+
+bool CoopSlots::try_acquire_all_for(int device, int timeout_ms) {
     std::unique_lock<std::mutex> lock(g_coop_mu);
-    bool &taken = g_coop_taken[device];
-    if (!g_coop_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms), [&] { return !taken; }))
+    unsigned long long &used = g_coop_used[device];
+    if (!g_coop_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms < 0 ? 0 : timeout_ms), [&] { return used == 0; }))
         return false;
-    taken = true;
+    used = ALL_TAKEN;
     return true;
 }
 
-void CoopSlots::release(int device) {
+void CoopSlots::release_all(int device) {
     {
         std::lock_guard<std::mutex> lock(g_coop_mu);
-        g_coop_taken[device] = false;
+        g_coop_used[device] = 0;
     }
     g_coop_cv.notify_all();
 }

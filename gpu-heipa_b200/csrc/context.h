@@ -186,34 +186,44 @@ struct Ctx {
 };
 
 // Cooperative launches (grids whose blocks wait for one another at grid
-// barriers) run one at a time per device. Concurrent solves (HM sub-solves,
-// batch and server requests) may each want one; two such grids that were
-// each only partly resident (the block scheduler spreads blocks over all
-// SMs, next to kernels of other streams) could wait at their barriers for
-// SMs that the other's waiting blocks hold. With one cooperative grid per
-// device, every other kernel on the device finishes without waiting for it,
-// so its remaining blocks are always scheduled. A launch takes the device's
-// slot here (waiting on the host while another grid holds it) and returns it
-// after its kernel has completed.
+// barriers) share a per-device budget of S blocks, S = the SM count.
+// Concurrent solves (HM sub-solves, batch and server requests) may each want
+// such a grid. A grid of b blocks takes min(b, S) of the budget and gives it
+// back after its kernel has completed; a grid of more than S blocks takes all
+// of it and runs alone (the cooperative launch itself checks that it fits).
+// Why this is enough: the grids holding budget have at most S blocks in all,
+// and every block fits on an SM that holds none of them (it launched at all).
+// While any of those blocks is still waiting to start, fewer than S SMs hold
+// blocks of these grids, so some SM holds none; the waiting block starts
+// there once the ordinary kernels on that SM end, and those never wait for
+// anything. So all blocks of all running grids become resident together, and
+// no grid waits at a barrier for SMs that another waiting grid holds.
 class CoopSlots {
 public:
-    static void acquire(int device);
-    // Waits at most timeout_ms; false when the slot stayed taken.
-    static bool try_acquire_for(int device, int timeout_ms);
-    static void release(int device);
+    // Takes min(blocks, budget) blocks of `device`'s budget (waiting while
+    // they are not free); budget = the device's SM count.
+    static void acquire(int device, u32 blocks, u32 budget);
+    static void release(int device, u32 blocks, u32 budget);
+    // The whole budget (no other cooperative grid runs); waits at most
+    // timeout_ms, false when it did not become free.
+    static bool try_acquire_all_for(int device, int timeout_ms);
+    static void release_all(int device);
 };
 
-// Holds the device's cooperative slot for the lifetime of the scope. The
-// destructor first waits for `stream` (errors ignored), so the slot is never
-// returned while the grid may still run, even when the scope is left by an
-// exception between the launch and the status read.
+// Holds `blocks` of the device's cooperative budget for the lifetime of the
+// scope. The destructor first waits for `stream` (errors ignored), so the
+// budget is never returned while the grid may still run, even when the scope
+// is left by an exception between the launch and the status read.
 struct CoopGuard {
     int device;
     cudaStream_t stream;
-    CoopGuard(int dev, cudaStream_t s) : device(dev), stream(s) { CoopSlots::acquire(dev); }
+    u32 blocks, budget;
+    CoopGuard(int dev, cudaStream_t s, u32 b, u32 sms) : device(dev), stream(s), blocks(b), budget(sms) {
+        CoopSlots::acquire(dev, blocks, budget);
+    }
     ~CoopGuard() {
         cudaStreamSynchronize(stream);
-        CoopSlots::release(device);
+        CoopSlots::release(device, blocks, budget);
     }
     CoopGuard(const CoopGuard &) = delete;
     CoopGuard &operator=(const CoopGuard &) = delete;

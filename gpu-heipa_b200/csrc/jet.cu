@@ -2863,12 +2863,12 @@ static void jet_refine_fused(Ctx &ctx, JetLevel &L, const std::vector<u32> &rati
     ctx.zero_counters();
     const size_t smem = 34 * (size_t) k * sizeof(s32);
     JArgs a = make_args(L);
-    std::optional<CoopGuard> coop;  // the device's cooperative slot, until the kernel has completed
+    std::optional<CoopGuard> coop;  // cooperative budget (grid blocks), until the kernel has completed
     if (blocks <= 1) {
         KernTimer kt(ctx, "k_jet_fused");
         k_jet_loop<false><<<1, FB, smem, ctx.stream>>>(a, F, d); note_launch();
     } else {
-        coop.emplace(ctx.device, ctx.stream);
+        coop.emplace(ctx.device, ctx.stream, blocks, (u32) ctx.sm_count);
         KernTimer kt(ctx, "k_jet_coop");
         void *args[] = {&a, &F, &d};
         HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_jet_loop<true>, dim3(blocks), dim3(FB), args, smem,

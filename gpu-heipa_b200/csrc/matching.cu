@@ -538,8 +538,8 @@ static u32 match_graph_impl(Ctx &ctx, const DGraph &g, u32 *mapping, bool allow_
         u32 cnt0 = n;
         u32 sd = seed;
         void *args[] = {&gg, &vcmap, &hn, &pl, &pl2, &cnt0, &claim, &heavy, &huge, &ctr, &sd, &bar, &err};
-        // the device's cooperative slot, held until the kernel has completed
-        CoopGuard coop(ctx.device, ctx.stream);
+        // cooperative budget (grid blocks), held until the kernel has completed
+        CoopGuard coop(ctx.device, ctx.stream, grid, (u32) ctx.sm_count);
         HP_CUDA(cudaLaunchCooperativeKernel((const void *) k_match_loop, dim3(grid), dim3(PICK_BLOCK), args, 0,
                                             ctx.stream));
         note_launch();

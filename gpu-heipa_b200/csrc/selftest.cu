@@ -52,7 +52,7 @@ extern "C" int hp_selftest_barrier_timeout(int device, uint32_t blocks, uint32_t
         void *args[] = {&bar, &err, &absent};
         hp::u32 h_err = 0;
         float t = 0.f;
-        hp::CoopGuard coop(device, s);  // the device's cooperative slot, until the kernel has completed
+        hp::CoopGuard coop(device, s, blocks, (hp::u32) sms);  // cooperative budget until the kernel has completed
         if (cudaMemsetAsync(d, 0, 4 * sizeof(hp::u32), s) != cudaSuccess || cudaEventRecord(e0, s) != cudaSuccess ||
             cudaLaunchCooperativeKernel((const void *) hp::k_barrier_selftest, dim3(blocks), dim3(32), args, 0, s) !=
                 cudaSuccess ||
@@ -74,10 +74,10 @@ extern "C" int hp_selftest_barrier_timeout(int device, uint32_t blocks, uint32_t
 }
 
 extern "C" int hp_coop_slot_acquire(int device, int timeout_ms) {
-    return hp::CoopSlots::try_acquire_for(device, timeout_ms) ? HP_OK : HP_ERR_BUSY;
+    return hp::CoopSlots::try_acquire_all_for(device, timeout_ms) ? HP_OK : HP_ERR_BUSY;
 }
 
 extern "C" int hp_coop_slot_release(int device) {
-    hp::CoopSlots::release(device);
+    hp::CoopSlots::release_all(device);
     return HP_OK;
 }

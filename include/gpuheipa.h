@@ -190,16 +190,19 @@ int hp_last_solve_level(const hp_ctx *ctx, uint32_t index, uint32_t *n, uint64_t
 #define HP_DEVERR_SPIN 8u
 int hp_selftest_barrier_timeout(int device, uint32_t blocks, uint32_t *err_bits, double *ms);
 
-/* Diagnostics of the cooperative-launch slot (host only, no device work).
+/* Diagnostics of the cooperative-launch budget (host only, no device work).
  * Grids whose blocks wait for one another at grid barriers (the cooperative
- * Jet level loop and matching loop, and the self-test above) run one at a
- * time per device: each launch takes the device's slot and returns it after
- * its kernel has completed, so two partly resident cooperative grids can
- * never wait for each other. hp_coop_slot_acquire takes the slot of `device`
- * (waiting at most timeout_ms; HP_ERR_BUSY when it stayed taken) and
- * hp_coop_slot_release returns it; a caller that holds the slot delays every
- * cooperative launch of this library on that device. No counterpart in the
- * reference (it runs one solve on one stream). */
+ * Jet level loop and matching loop, and the self-test above) share a budget
+ * of as many blocks as the device has SMs: a grid of b blocks holds min(b,
+ * budget) of it until its kernel has completed, and a larger grid holds all
+ * of it. The grids running together then have at most one block per SM in
+ * all, so they always become resident together and never wait for each
+ * other. hp_coop_slot_acquire takes the whole budget of `device` (waiting at
+ * most timeout_ms for every running cooperative grid to finish; HP_ERR_BUSY
+ * when that did not happen) and hp_coop_slot_release returns it; a caller
+ * that holds it delays every cooperative launch of this library on that
+ * device. No counterpart in the reference (it runs one solve on one
+ * stream). */
 int hp_coop_slot_acquire(int device, int timeout_ms);
 int hp_coop_slot_release(int device);
 
