@@ -300,8 +300,16 @@ __device__ __forceinline__ u32 range_hash(u32 key, u32 size) {
     return (u32) (((u64) (key * 2654435761u) * (u64) size) >> 32);
 }
 
+// One global hash table per huge cluster; a slot is (key, weight) in one
+// 8-byte word pair, so an insert touches one cache line (the tables of the
+// hub clusters of a large level do not fit in L2).
+struct HugeSlot {
+    u32 key;
+    s32 w;
+};
+
 __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u32 *hl, const u32 *hcnt,
-                                                               const u32 *hoff, u32 *tkeys, s32 *twts) {
+                                                               const u32 *hoff, HugeSlot *slots) {
     __shared__ u32 scan_sm[32];
     const u32 total = *hcnt;
     unsigned long long msum = 0;
@@ -309,12 +317,8 @@ __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u
         const u32 c = hl[i];
         const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
         const u32 tsz = 2 * cap;
-        u32 *tk = tkeys + hoff[c];
-        s32 *tw = twts + hoff[c];
-        for (u32 s = threadIdx.x; s < tsz; s += blockDim.x) {
-            tk[s] = EMPTY;
-            tw[s] = 0;
-        }
+        HugeSlot *tb = slots + hoff[c];
+        for (u32 s = threadIdx.x; s < tsz; s += blockDim.x) tb[s] = HugeSlot{EMPTY, 0};
         __syncthreads();
         for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
             const u32 u = a.mlist[mi];
@@ -327,9 +331,9 @@ __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u
                 u32 h = range_hash(cv, tsz);
                 bool ok = false;
                 for (u32 probe = 0; probe < tsz; ++probe) {
-                    const u32 prev = atomicCAS(&tk[h], EMPTY, cv);
+                    const u32 prev = atomicCAS(&tb[h].key, EMPTY, cv);
                     if (prev == EMPTY || prev == cv) {
-                        atomicAdd(&tw[h], w);
+                        atomicAdd(&tb[h].w, w);
                         ok = true;
                         break;
                     }
@@ -344,12 +348,13 @@ __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u
         u32 cntu = 0;
         for (u32 s0 = 0; s0 < tsz; s0 += blockDim.x) {
             const u32 s = s0 + threadIdx.x;
-            const bool has = s < tsz && tk[s] != EMPTY;
+            const HugeSlot sl = s < tsz ? tb[s] : HugeSlot{EMPTY, 0};
+            const bool has = sl.key != EMPTY;
             u32 tot;
             const u32 p = block_exclusive_scan<u32>(has ? 1u : 0u, tot, scan_sm);
             if (has) {
-                a.c.adj[out + cntu + p] = tk[s];
-                a.c.ew[out + cntu + p] = tw[s];
+                a.c.adj[out + cntu + p] = sl.key;
+                a.c.ew[out + cntu + p] = sl.w;
             }
             cntu += tot;
         }
@@ -444,12 +449,11 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
         HP_LAUNCH_CHECK();
     }
     if (nh) {
-        u32 *tkeys = ctx.balloc<u32>(hslots);
-        s32 *twts = ctx.balloc<s32>(hslots);
+        HugeSlot *slots = ctx.balloc<HugeSlot>(hslots);
         KernTimer kt(ctx, "contract");
         KernTimer kt1(ctx, "contract_huge");
         k_contract_huge<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
-            a, hl, &st->cnt[2], hoffc, tkeys, twts); note_launch();
+            a, hl, &st->cnt[2], hoffc, slots); note_launch();
         HP_LAUNCH_CHECK();
     }
     const DevStatus &s2 = ctx.read_status();
