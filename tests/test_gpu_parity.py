@@ -52,9 +52,11 @@ def test_contract_parity(ctx, name, g):
     np.testing.assert_array_equal(cg.vw, ov)
 
 
-@pytest.mark.parametrize("group", [3, 4, 7])
+@pytest.mark.parametrize("group", [3, 4, 7, 512, 2048])
 def test_contract_parity_large_clusters(ctx, group):
-    # a caller-given mapping with clusters of more than two members
+    # a caller-given mapping with clusters of more than two members (512 and
+    # 2048 members: clusters of thousands of entries, the huge tier with its
+    # rows cut into work units of many members)
     g = H.Graph.rmat(12, 8, seed=9)
     mapping = (np.arange(g.n) // group).astype(np.uint32)
     n_c = int(mapping.max()) + 1
