@@ -23,7 +23,6 @@ constexpr u32 C_BLOCK_SMALL_BITS = 11;
 constexpr int C_WARP_BLOCK = 128;  // 4 warps per block for the warp kernel
 constexpr int C_HUGE_BLOCK = 1024;
 constexpr int C_ST_BLOCK_LARGE = 3;  // status slot: clusters of the large block tier
-constexpr int C_ST_HUGE_UNITS = 4;   // status slot: work units of the huge tier
 
 __device__ __forceinline__ u32 hslot(u32 key, u32 bits) { return (key * 2654435761u) >> (32 - bits); }
 
@@ -309,91 +308,32 @@ struct HugeSlot {
     s32 w;
 };
 
-// Huge clusters (rows of more than C_BLOCK_MAX entries) are aggregated by the
-// whole GPU instead of one block each (a block per cluster left most SMs
-// idle while the largest hub clusters finished): the tables are cleared, every
-// member row is cut into HUGE_UNIT-entry work units that any block takes, all
-// units of a cluster insert into its table with atomics, and a last pass
-// compacts every table into its coarse row. The slot order of a row depends on
-// the insertion order, like the other tiers' rows; every consumer of a coarse
-// row is independent of its order.
-constexpr u32 HUGE_UNIT = 4096;
-
-__global__ void k_huge_clear(HugeSlot *slots, u64 n) {
-    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (u64) gridDim.x * blockDim.x)
-        slots[i] = HugeSlot{EMPTY, 0};
-}
-
-// One warp per huge cluster: its lanes walk the members and append one unit
-// (member position in mlist << 32 | chunk) per HUGE_UNIT entries of each row.
-__global__ void __launch_bounds__(BLOCK) k_huge_units(CArgs a, const u32 *hl, const u32 *hcnt,
-                                                       unsigned long long *units, u32 units_cap, u32 *units_cnt) {
+__global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u32 *hl, const u32 *hcnt,
+                                                               const u32 *hoff, HugeSlot *slots) {
+    __shared__ u32 scan_sm[32];
     const u32 total = *hcnt;
-    const u32 warps = (gridDim.x * blockDim.x) >> 5;
-    for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
+    unsigned long long msum = 0;
+    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
         const u32 c = hl[i];
-        const u32 m0 = a.moff[c], m1 = a.moff[c + 1];
-        for (u32 b = m0; b < m1; b += 32) {
-            const u32 mi = b + lane_id();
-            const u32 nch = mi < m1 ? (a.g.rowlen[a.mlist[mi]] + HUGE_UNIT - 1) / HUGE_UNIT : 0u;
-            u32 incl = nch;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const u32 y = __shfl_up_sync(FULL, incl, o);
-                if (lane_id() >= o) incl += y;
-            }
-            const u32 wtot = __shfl_sync(FULL, incl, 31);
-            u32 base = 0;
-            if (lane_id() == 31 && wtot) base = atomicAdd(units_cnt, wtot);
-            base = __shfl_sync(FULL, base, 31);
-            for (u32 j = 0; j < nch; ++j) {
-                const u32 at = base + incl - nch + j;
-                if (at < units_cap) units[at] = ((unsigned long long) mi << 32) | j;
-                else set_error(a.err, DEV_ERR_HASH_FULL);
-            }
-        }
-    }
-}
-
-// One block per work unit: inserts the unit's entries into its cluster's
-// table (linear probing, key CAS then weight add), four entries per thread
-// loaded before their coarse ids are gathered.
-__global__ void __launch_bounds__(BLOCK) k_huge_insert(CArgs a, const u32 *hoff, HugeSlot *slots,
-                                                        const unsigned long long *units, const u32 *units_cnt,
-                                                        u32 units_cap) {
-    u32 total = *units_cnt;
-    if (total > units_cap) total = units_cap;
-    for (u32 wi = blockIdx.x; wi < total; wi += gridDim.x) {
-        const unsigned long long it = units[wi];
-        const u32 u = a.mlist[(u32) (it >> 32)];
-        const u32 c = a.map[u];
-        const u32 len = a.g.rowlen[u];
-        const u32 lo = (u32) it * HUGE_UNIT;
-        const u32 hi = len - lo < HUGE_UNIT ? len : lo + HUGE_UNIT;
-        const u64 beg = a.g.rowptr[u];
-        const u32 tsz = 2 * (a.c.rowptr[c + 1] - a.c.rowptr[c]);
+        const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
+        const u32 tsz = 2 * cap;
         HugeSlot *tb = slots + hoff[c];
-        for (u32 t0 = lo + threadIdx.x; t0 < hi; t0 += 4 * blockDim.x) {
-            u32 cv[4];
-            s32 w[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const u32 t = t0 + j * blockDim.x;
-                cv[j] = t < hi ? __ldg(&a.g.adj[beg + t]) : EMPTY;
-                w[j] = t < hi ? g_ew(a.g, beg + t) : 0;
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (cv[j] != EMPTY) cv[j] = __ldg(&a.map[cv[j]]);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                if (cv[j] == EMPTY || cv[j] == c) continue;
-                u32 h = range_hash(cv[j], tsz);
+        for (u32 s = threadIdx.x; s < tsz; s += blockDim.x) tb[s] = HugeSlot{EMPTY, 0};
+        __syncthreads();
+        for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
+            const u32 u = a.mlist[mi];
+            const u64 beg = a.g.rowptr[u];
+            const u32 len = a.g.rowlen[u];
+            for (u32 t = threadIdx.x; t < len; t += blockDim.x) {
+                const u32 cv = a.map[a.g.adj[beg + t]];
+                if (cv == c) continue;
+                const s32 w = g_ew(a.g, beg + t);
+                u32 h = range_hash(cv, tsz);
                 bool ok = false;
                 for (u32 probe = 0; probe < tsz; ++probe) {
-                    const u32 prev = atomicCAS(&tb[h].key, EMPTY, cv[j]);
-                    if (prev == EMPTY || prev == cv[j]) {
-                        atomicAdd(&tb[h].w, w[j]);
+                    const u32 prev = atomicCAS(&tb[h].key, EMPTY, cv);
+                    if (prev == EMPTY || prev == cv) {
+                        atomicAdd(&tb[h].w, w);
                         ok = true;
                         break;
                     }
@@ -402,24 +342,13 @@ __global__ void __launch_bounds__(BLOCK) k_huge_insert(CArgs a, const u32 *hoff,
                 if (!ok) set_error(a.err, DEV_ERR_HASH_FULL);
             }
         }
-    }
-}
-
-// One block per huge cluster: compacts its table into the coarse row.
-__global__ void __launch_bounds__(C_HUGE_BLOCK) k_huge_emit(CArgs a, const u32 *hl, const u32 *hcnt, const u32 *hoff,
-                                                           const HugeSlot *slots) {
-    __shared__ u32 scan_sm[32];
-    const u32 total = *hcnt;
-    unsigned long long msum = 0;
-    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
-        const u32 c = hl[i];
-        const u32 tsz = 2 * (a.c.rowptr[c + 1] - a.c.rowptr[c]);
-        const HugeSlot *tb = slots + hoff[c];
+        __syncthreads();
+        // emit in chunks of blockDim.x slots
         const u64 out = a.c.rowptr[c];
         u32 cntu = 0;
         for (u32 s0 = 0; s0 < tsz; s0 += blockDim.x) {
-            const u32 sidx = s0 + threadIdx.x;
-            const HugeSlot sl = sidx < tsz ? tb[sidx] : HugeSlot{EMPTY, 0};
+            const u32 s = s0 + threadIdx.x;
+            const HugeSlot sl = s < tsz ? tb[s] : HugeSlot{EMPTY, 0};
             const bool has = sl.key != EMPTY;
             u32 tot;
             const u32 p = block_exclusive_scan<u32>(has ? 1u : 0u, tot, scan_sm);
@@ -521,19 +450,9 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     }
     if (nh) {
         HugeSlot *slots = ctx.balloc<HugeSlot>(hslots);
-        // work units: at most one per HUGE_UNIT entries of each member row
-        const u64 units_cap64 = hslots / (2 * (u64) HUGE_UNIT) + g.n + 1;
-        const u32 units_cap = (u32) std::min<u64>(units_cap64, 0xFFFFFFFFull);
-        unsigned long long *units = ctx.balloc<unsigned long long>(units_cap);
-        u32 *units_cnt = &st->cnt[C_ST_HUGE_UNITS];
         KernTimer kt(ctx, "contract");
         KernTimer kt1(ctx, "contract_huge");
-        k_huge_clear<<<ctx.grid(hslots, BLOCK), BLOCK, 0, ctx.stream>>>(slots, hslots); note_launch();
-        k_huge_units<<<ctx.grid((u64) nh * 32, BLOCK), BLOCK, 0, ctx.stream>>>(a, hl, &st->cnt[2], units, units_cap,
-                                                                              units_cnt); note_launch();
-        k_huge_insert<<<(u32) ctx.sm_count * 8, BLOCK, 0, ctx.stream>>>(a, hoffc, slots, units, units_cnt,
-                                                                         units_cap); note_launch();
-        k_huge_emit<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
+        k_contract_huge<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
             a, hl, &st->cnt[2], hoffc, slots); note_launch();
         HP_LAUNCH_CHECK();
     }
