@@ -820,7 +820,21 @@ __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou,
     return acc;
 }
 
-template<bool NC = true, int B = 4>
+// Loads B row entries (ids and weights) strided by nthreads from t0.
+template<int B>
+__device__ __forceinline__ void load_entries(const JArgs &a, u64 beg, u32 t0, u32 to, u32 nthreads, u32 (&v)[B],
+                                             s32 (&w)[B]) {
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+        const u32 t = t0 + j * nthreads;
+        v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
+        w[j] = t < to ? g_ew(a.g, beg + t) : 0;
+    }
+}
+
+// With PF, the next batch's row entries are loaded before the current
+// batch's label gathers, so the row read and the gathers overlap.
+template<bool NC = true, int B = 4, bool PF = false>
 __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 nthreads,
                                                  bool inval, bool hub_upd = false) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
@@ -829,15 +843,32 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
     const u32 nu = x & ~MOVED;
     const u32 ou = um ? ldj<NC>(&a.dest_part[u]) : nu;
     long long acc = 0;
+    if (PF) {
+        u32 t0 = from + tid;
+        if (t0 >= to) return 0;
+        u32 v[B];
+        s32 w[B];
+        load_entries<B>(a, beg, t0, to, nthreads, v, w);
+        for (;;) {
+            const u32 t1 = t0 + B * nthreads;
+            u32 vn[B];
+            s32 wn[B];
+            load_entries<B>(a, beg, t1, to, nthreads, vn, wn);
+            acc += delta_batch<B, NC>(a, nu, ou, um, v, w, inval, hub_upd);
+            if (t1 >= to) break;
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                v[j] = vn[j];
+                w[j] = wn[j];
+            }
+            t0 = t1;
+        }
+        return acc;
+    }
     for (u32 t0 = from + tid; t0 < to; t0 += B * nthreads) {
         u32 v[B];
         s32 w[B];
-#pragma unroll
-        for (int j = 0; j < B; ++j) {
-            const u32 t = t0 + j * nthreads;
-            v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
-            w[j] = t < to ? g_ew(a.g, beg + t) : 0;
-        }
+        load_entries<B>(a, beg, t0, to, nthreads, v, w);
         acc += delta_batch<B, NC>(a, nu, ou, um, v, w, inval, hub_upd);
     }
     return acc;
@@ -952,7 +983,7 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
 // is added with one atomic per warp, so no warp waits for the others of its
 // block at the end.
 template<int B>
-__global__ void __launch_bounds__(BLOCK, B > 4 ? 4 : 6) k_delta_chunk(JArgs a) {
+__global__ void __launch_bounds__(BLOCK, B > 4 ? 4 : 5) k_delta_chunk(JArgs a) {
     u32 total = a.st->cnt[ST_HEAVY];
     if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
@@ -962,7 +993,7 @@ __global__ void __launch_bounds__(BLOCK, B > 4 ? 4 : 6) k_delta_chunk(JArgs a) {
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         u32 u, from, to, nch;
         chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
-        acc += delta_range<true, B>(a, u, from, to, lane_id(), 32, inval, hub_upd);
+        acc += delta_range<true, B, B <= 4>(a, u, from, to, lane_id(), 32, inval, hub_upd);
     }
     acc = warp_sum<long long>(acc);
     if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
