@@ -162,6 +162,18 @@ __device__ __forceinline__ T ldj(const T *p) {
     return NC ? __ldg(p) : *p;
 }
 
+// Loads B row entries (ids and weights) strided by nthreads from t0.
+template<int B>
+__device__ __forceinline__ void load_entries(const JArgs &a, u64 beg, u32 t0, u32 to, u32 nthreads, u32 (&v)[B],
+                                             s32 (&w)[B]) {
+#pragma unroll
+    for (int j = 0; j < B; ++j) {
+        const u32 t = t0 + j * nthreads;
+        v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;  // SENTINEL == EMPTY
+        w[j] = t < to ? g_ew(a.g, beg + t) : 0;
+    }
+}
+
 __device__ __forceinline__ u32 thash(u32 key, u32 mask) { return (key * 2654435761u >> 7) & mask; }
 
 __device__ __forceinline__ u32 table_mask_for(u32 len, u32 k, u32 cap) {
@@ -229,6 +241,37 @@ template<bool BLK, bool NC = true>
 __device__ __forceinline__ void dtable_build_range(const JArgs &a, u32 u, s32 *tv, u32 from, u32 len) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     const u32 gs = Grp<BLK>::size(), tid = Grp<BLK>::tid();
+    if (NC) {
+        // kernels that do not write labels: the next four entries are loaded
+        // while the current four labels are gathered
+        u32 t0 = from + tid;
+        if (t0 < len) {
+            u32 b[4];
+            s32 w[4];
+            load_entries<4>(a, beg, t0, len, gs, b, w);
+            for (;;) {
+                const u32 t1 = t0 + 4 * gs;
+                u32 bn[4];
+                s32 wn[4];
+                load_entries<4>(a, beg, t1, len, gs, bn, wn);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (b[j] != EMPTY) b[j] = ldj<NC>(&a.map[b[j]]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (b[j] != EMPTY) atomicAdd(&tv[b[j]], w[j]);
+                if (t1 >= len) break;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    b[j] = bn[j];
+                    w[j] = wn[j];
+                }
+                t0 = t1;
+            }
+        }
+        Grp<BLK>::sync();
+        return;
+    }
     for (u32 t0 = from + tid; t0 < len; t0 += 4 * gs) {
         u32 b[4];
         s32 w[4];
@@ -624,65 +667,93 @@ __global__ void __launch_bounds__(BLOCK) k_lp_filter(JArgs a) {
     }
 }
 
-// afterburner (:269-331 / ProMap :273-320): contribution of neighbour v.
+// afterburner (:269-331 / ProMap :273-320): the terms of four loaded row
+// entries of u (v = SENTINEL marks an empty slot).
+template<bool NC>
+__device__ __forceinline__ s32 ab_batch(const JArgs &a, u32 u, s32 ug, u32 ou, u32 nu, const u32 (&v)[4],
+                                        const s32 (&w)[4]) {
+    u32 nv[4], ov[4];
+    s32 vg[4];
+    // only neighbours that move first (higher gain, or equal gain and a
+    // lower id) contribute: their target and label come with the gain in
+    // one record (abrec) or are gathered after the gains
+    bool first[4];
+    if (a.abrec) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const unsigned long long r = v[j] != SENTINEL ? ldj<NC>(&a.abrec[v[j]]) : 0ull;
+            vg[j] = (s32) (u32) r;
+            nv[j] = (u32) (r >> 32) & 0xFFFFu;
+            ov[j] = (u32) (r >> 48);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) vg[j] = v[j] != SENTINEL ? ldj<NC>(&a.gain1[v[j]]) : 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
+            if (first[j]) {
+                nv[j] = ldj<NC>(&a.dest_part[v[j]]);
+                ov[j] = ldj<NC>(&a.map[v[j]]);
+            }
+        }
+    }
+    s32 change = 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        if (!first[j]) continue;
+        s32 t;
+        if (!a.code) {
+            t = wmul(w[j], (s32) (nv[j] == nu) - (s32) (nv[j] == ou) + (s32) (ov[j] == ou) - (s32) (ov[j] == nu));
+        } else {
+            const s32 before_u = wsub(D(a, ou, ov[j]), D(a, nu, ov[j]));
+            const s32 after_u = wsub(D(a, ou, nv[j]), D(a, nu, nv[j]));
+            t = wmul(w[j], wsub(after_u, before_u));
+        }
+        change = wadd(change, t);
+    }
+    return change;
+}
 
 // Sum of the afterburner terms over entries [from, to) of u's row, strided
 // over a group of threads (wrap-around s32 arithmetic). The gains, targets
 // and labels read here are not written by the afterburner kernels, so they
-// are gathered through the non-coherent path, four entries at a time.
-template<bool NC = true>
+// are gathered through the non-coherent path, four entries at a time; with
+// PF the next four row entries are loaded while those are gathered.
+template<bool NC = true, bool PF = false>
 __device__ __forceinline__ s32 ab_range(const JArgs &a, u32 u, s32 ug, u32 ou, u32 nu, u32 from, u32 to, u32 tid,
                                         u32 nthreads) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     s32 change = 0;
+    if (PF) {
+        u32 t0 = from + tid;
+        if (t0 >= to) return 0;
+        u32 v[4];
+        s32 w[4];
+        load_entries<4>(a, beg, t0, to, nthreads, v, w);
+        for (;;) {
+            const u32 t1 = t0 + 4 * nthreads;
+            u32 vn[4];
+            s32 wn[4];
+            load_entries<4>(a, beg, t1, to, nthreads, vn, wn);
+            change = wadd(change, ab_batch<NC>(a, u, ug, ou, nu, v, w));
+            if (t1 >= to) break;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                v[j] = vn[j];
+                w[j] = wn[j];
+            }
+            t0 = t1;
+        }
+        return change;
+    }
     for (u32 t0 = from + tid; t0 < to; t0 += 4 * nthreads) {
-        u32 v[4], nv[4], ov[4];
-        s32 w[4], vg[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const u32 t = t0 + j * nthreads;
-            v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
-            w[j] = t < to ? g_ew(a.g, beg + t) : 0;
-        }
-        // only neighbours that move first (higher gain, or equal gain and a
-        // lower id) contribute: their target and label come with the gain in
-        // one record (abrec) or are gathered after the gains
-        bool first[4];
-        if (a.abrec) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const unsigned long long r = v[j] != SENTINEL ? ldj<NC>(&a.abrec[v[j]]) : 0ull;
-                vg[j] = (s32) (u32) r;
-                nv[j] = (u32) (r >> 32) & 0xFFFFu;
-                ov[j] = (u32) (r >> 48);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) vg[j] = v[j] != SENTINEL ? ldj<NC>(&a.gain1[v[j]]) : 0;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                first[j] = v[j] != SENTINEL && (vg[j] > ug || (vg[j] == ug && v[j] < u));
-                if (first[j]) {
-                    nv[j] = ldj<NC>(&a.dest_part[v[j]]);
-                    ov[j] = ldj<NC>(&a.map[v[j]]);
-                }
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            if (!first[j]) continue;
-            s32 t;
-            if (!a.code) {
-                t = wmul(w[j], (s32) (nv[j] == nu) - (s32) (nv[j] == ou) + (s32) (ov[j] == ou) - (s32) (ov[j] == nu));
-            } else {
-                const s32 before_u = wsub(D(a, ou, ov[j]), D(a, nu, ov[j]));
-                const s32 after_u = wsub(D(a, ou, nv[j]), D(a, nu, nv[j]));
-                t = wmul(w[j], wsub(after_u, before_u));
-            }
-            change = wadd(change, t);
-        }
+        u32 v[4];
+        s32 w[4];
+        load_entries<4>(a, beg, t0, to, nthreads, v, w);
+        change = wadd(change, ab_batch<NC>(a, u, ug, ou, nu, v, w));
     }
     return change;
 }
@@ -719,7 +790,7 @@ __global__ void __launch_bounds__(BLOCK) k_ab_thread(JArgs a) {
 // row of several chunks each warp adds its partial sum to abacc[u] and the
 // last warp to finish (counted in abcnt[u], after a fence) decides and resets
 // both words, so nothing waits for another warp.
-__global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
+__global__ void __launch_bounds__(BLOCK, 4) k_ab_chunk(JArgs a) {
     u32 total = a.st->cnt[ST_HEAVY];
     if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
@@ -728,7 +799,7 @@ __global__ void __launch_bounds__(BLOCK, 5) k_ab_chunk(JArgs a) {
         chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
         const s32 ug = __ldg(&a.gain1[u]);
         const u32 ou = __ldg(&a.map[u]), nu = __ldg(&a.dest_part[u]);
-        const s32 change = (s32) warp_sum<u32>((u32) ab_range(a, u, ug, ou, nu, from, to, lane_id(), 32));
+        const s32 change = (s32) warp_sum<u32>((u32) ab_range<true, true>(a, u, ug, ou, nu, from, to, lane_id(), 32));
         if (lane_id() == 0) {
             bool decide = nch == 1;
             s32 tot = change;
@@ -818,18 +889,6 @@ __device__ __forceinline__ long long delta_batch(const JArgs &a, u32 nu, u32 ou,
             if (v[j] != SENTINEL) a.dest_cache[v[j]] = NULL_PART;
     }
     return acc;
-}
-
-// Loads B row entries (ids and weights) strided by nthreads from t0.
-template<int B>
-__device__ __forceinline__ void load_entries(const JArgs &a, u64 beg, u32 t0, u32 to, u32 nthreads, u32 (&v)[B],
-                                             s32 (&w)[B]) {
-#pragma unroll
-    for (int j = 0; j < B; ++j) {
-        const u32 t = t0 + j * nthreads;
-        v[j] = t < to ? __ldg(&a.g.adj[beg + t]) : SENTINEL;
-        w[j] = t < to ? g_ew(a.g, beg + t) : 0;
-    }
 }
 
 // With PF, the next batch's row entries are loaded before the current
