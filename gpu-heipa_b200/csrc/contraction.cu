@@ -150,6 +150,29 @@ __global__ void k_contract_small(CArgs a, TierLists L) {
 // coarse neighbour cv differs from c; entries are strided over a group of
 // `nt` threads starting at `tid` across the concatenated member rows (one or
 // two members), four entries per thread loaded before they are inserted.
+// Loads four entries t0, t0 + nt, ... of the concatenated rows [b0, b0 + l0)
+// and [b1, b1 + l1) (total = l0 + l1); empty slots get EMPTY.
+__device__ __forceinline__ void load_pair_entries(const CArgs &a, u64 b0, u32 l0, u64 b1, u32 total, u32 t0, u32 nt,
+                                                  u32 (&cv)[4], s32 (&w)[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const u32 t = t0 + j * nt;
+        cv[j] = EMPTY;
+        w[j] = 0;
+        if (t < total) {
+            const u64 e = t < l0 ? b0 + t : b1 + (t - l0);
+            cv[j] = __ldg(&a.g.adj[e]);
+            w[j] = g_ew(a.g, e);
+        }
+    }
+}
+
+// Calls insert(cv, w) for every entry of the member rows of cluster c whose
+// coarse neighbour cv differs from c; entries are strided over a group of
+// `nt` threads starting at `tid` across the concatenated member rows (one or
+// two members at a time), four entries per thread loaded before their coarse
+// ids are gathered, and the next four loaded while those are gathered and
+// inserted.
 template<typename Insert>
 __device__ __forceinline__ void for_cluster_entries(const CArgs &a, u32 c, u32 tid, u32 nt, Insert insert) {
     const u32 m0 = a.moff[c], mc = a.moff[c + 1] - m0;
@@ -159,26 +182,29 @@ __device__ __forceinline__ void for_cluster_entries(const CArgs &a, u32 c, u32 t
         const u64 b0 = a.g.rowptr[u0], b1 = a.g.rowptr[u1];
         const u32 l0 = a.g.rowlen[u0], l1 = mi + 1 < mc ? a.g.rowlen[u1] : 0u;
         const u32 total = l0 + l1;
-        for (u32 t0 = tid; t0 < total; t0 += 4 * nt) {
-            u32 cv[4];
-            s32 w[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const u32 t = t0 + j * nt;
-                cv[j] = EMPTY;
-                w[j] = 0;
-                if (t < total) {
-                    const u64 e = t < l0 ? b0 + t : b1 + (t - l0);
-                    cv[j] = __ldg(&a.g.adj[e]);
-                    w[j] = g_ew(a.g, e);
-                }
-            }
+        u32 t0 = tid;
+        if (t0 >= total) continue;
+        u32 cv[4];
+        s32 w[4];
+        load_pair_entries(a, b0, l0, b1, total, t0, nt, cv, w);
+        for (;;) {
+            const u32 t1 = t0 + 4 * nt;
+            u32 cvn[4];
+            s32 wn[4];
+            load_pair_entries(a, b0, l0, b1, total, t1, nt, cvn, wn);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 if (cv[j] != EMPTY) cv[j] = __ldg(&a.map[cv[j]]);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 if (cv[j] != EMPTY && cv[j] != c) insert(cv[j], w[j]);
+            if (t1 >= total) break;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                cv[j] = cvn[j];
+                w[j] = wn[j];
+            }
+            t0 = t1;
         }
     }
 }
@@ -320,6 +346,8 @@ __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u
         HugeSlot *tb = slots + hoff[c];
         for (u32 s = threadIdx.x; s < tsz; s += blockDim.x) tb[s] = HugeSlot{EMPTY, 0};
         __syncthreads();
+        // one entry per thread at a time: batching four entries here (as the
+        // other tiers do) measured slower, the table atomics then dominate
         for (u32 mi = a.moff[c]; mi < a.moff[c + 1]; ++mi) {
             const u32 u = a.mlist[mi];
             const u64 beg = a.g.rowptr[u];
