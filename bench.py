@@ -77,7 +77,7 @@ WORKLOADS = {
 ROOFLINE_KERNELS = ("contract", "jet_gain", "k_delta")
 # every kernel timer of the library (printed with --kernel-timers)
 KERNEL_TIMERS = ("contract", "contract_thread", "contract_warp", "contract_block", "contract_huge", "jet_gain", "k_lp_dispatch", "k_lp_warp", "k_lp_block", "k_lp_filter", "k_afterburner",
-                 "k_ab_thread", "k_ab_chunk", "k_apply", "k_delta", "k_delta_thread", "k_delta_chunk",
+                 "k_ab_thread", "k_ab_chunk", "k_apply", "k_delta", "k_delta_thread", "k_delta_chunk", "k_hub_rebuild",
                  "k_weak_pick", "k_weak_dispatch", "k_weak_warp", "k_weak_block", "k_strong_pick",
                  "k_strong_dispatch", "k_strong_warp", "k_strong_block")
 

@@ -87,20 +87,20 @@ struct JArgs {
     // dest_part (next 16) and label (top 16) of a vertex, written by the
     // filter, so that a neighbour costs one gather. Null: separate arrays.
     unsigned long long *abrec;
-    // Tracked hub connectivity (k <= HUB_K, hub_stale set): hubacc then
+    // Tracked hub connectivity (k <= HUB_K, hub_cur set): hubacc then
     // holds, for every hub row h and block b, the row's connection to b at
     // hubacc[h * k + b] (the two counters one moved neighbour changes share a
     // cache line; a block-major layout measured slower), kept up to date by
     // the delta pass. Without tracking, hub rows are rescanned in chunks on
     // every pass.
     // A perform whose moved rows hold more than hub_track_max entries does
-    // not update the hub sums but sets *hub_stale; the next pass that reads
-    // them first rebuilds them from the hub rows (hub_items: chunk items of
-    // all hub rows, hub_vertex: the row of each hub slot).
+    // not update the hub sums but advances the generation *hub_cur; a pass
+    // that needs the sums of a hub whose generation (hub_gen) is older
+    // rebuilds that hub's sums from its row first (hub_vertex: the row of
+    // each hub slot). hub_cur is null without tracking.
     unsigned long long hub_track_max;
-    u32 *hub_stale;
-    const unsigned long long *hub_items;
-    u32 hub_nitems;
+    u32 *hub_cur;
+    u32 *hub_gen;
     const u32 *hub_vertex;
     s32 *abacc;  // afterburner partial sums of multi-chunk rows (zero between uses)
     u32 *abcnt;  // afterburner finished chunks of multi-chunk rows (zero between uses)
@@ -562,6 +562,31 @@ __device__ __forceinline__ void emit_hub_chunks(const JArgs &a, u32 h, u32 len) 
     warp_emit_chunks(a, h, nch, &a.st->cnt[ST_CHUNKS]);
 }
 
+// Hub rows met by a table pass's dispatch (warp-collective; `hub` marks hub
+// row u, list slot s2). Without tracking, every hub row is cut into chunk
+// items for k_hub. With tracking, a hub whose sums are older than the current
+// generation gets its sums zeroed, its generation advanced and its chunk items
+// emitted for k_hub_rebuild, which runs before the pass reads the sums; hubs
+// the pass does not need are left as they are.
+__device__ __forceinline__ void hub_dispatch(const JArgs &a, u32 s2, bool hub, u32 u) {
+    if (!a.hubacc) return;
+    if (!a.hub_cur) {
+        emit_hub_chunks(a, s2, hub ? a.g.rowlen[u] : 0u);
+        return;
+    }
+    u32 h = 0, len = 0;
+    if (hub) {
+        h = (u32) (a.dlab[u] >> DL_SLOT_SHIFT) - 1u;  // k_hub_tracked reports a row without a slot
+        const u32 cur = *a.hub_cur;
+        if (h < a.hub_cap && a.hub_gen[h] != cur) {
+            a.hub_gen[h] = cur;
+            for (u32 b = 0; b < a.k; ++b) a.hubacc[(u64) h * a.k + b] = 0;
+            len = a.g.rowlen[u];
+        }
+    }
+    emit_hub_chunks(a, h, len);
+}
+
 __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
     const u64 stride = (u64) gridDim.x * blockDim.x;
     u32 nrec = 0;
@@ -579,7 +604,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
                 cls = table_tier(len, a.k, a.hubacc ? a.hub_deg : JW_DEG);
                 // a tracked hub row is not scanned: it reads its k sums
                 // (counted as k / 3 entries of 12 bytes)
-                erec += (cls == 2 && a.hub_stale) ? (a.k + 2) / 3 : len;
+                erec += (cls == 2 && a.hub_cur) ? (a.k + 2) / 3 : len;
                 if (cls == 0) lp_thread(a, u, ratio);
             }
         }
@@ -587,7 +612,7 @@ __global__ void __launch_bounds__(BLOCK) k_lp_dispatch(JArgs a, u32 ratio) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
-        if (a.hubacc && !a.hub_stale) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
+        hub_dispatch(a, s2, cls == 2, u);
     }
     block_count(&a.st->cnt[ST_AUX], (unsigned long long *) &a.st->sum[4], nrec, erec);
 }
@@ -834,10 +859,11 @@ __global__ void __launch_bounds__(BLOCK, 4) k_ab_chunk(JArgs a) {
 // marks an empty slot) of a row whose vertex has new label nu and old label
 // ou (um: it changed block). All B labels are gathered, then the old labels
 // of moved neighbours, so B dependent gathers are in flight at a time.
-// Whether this perform updates the tracked hub sums (else it marks them
-// stale): read by every delta kernel after k_apply has counted the entries.
+// Whether this perform updates the tracked hub sums (else it advances their
+// generation, so that every hub's sums count as stale): read by every delta
+// kernel after k_apply has counted the entries.
 __device__ __forceinline__ bool hub_update_now(const JArgs &a) {
-    return a.hub_stale && (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] <= a.hub_track_max;
+    return a.hub_cur && (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] <= a.hub_track_max;
 }
 
 template<int B, bool NC>
@@ -956,11 +982,14 @@ __device__ __forceinline__ long long delta_staged(const JArgs &a, u32 u, const u
     return acc;
 }
 
-// When the moved rows hold at least inval_all_min entries, nearly every cache
-// is invalidated anyway: the delta kernels then skip the scattered resets and
-// k_inval_unmark resets all caches with one sequential fill. Only enabled where a
-// recomputed gain equals the cached one for every vertex whose neighbourhood
-// did not change (a fixed filter ratio per level, or the mapping objective).
+// When the moved rows hold at least inval_all_min entries (a percentage of the
+// level's entries, Tunables::jet_inval_all_pct), most caches are invalidated
+// anyway (on an R-MAT level, moved rows with 5% of the entries reach nearly
+// every vertex): the delta kernels then skip the scattered resets, one 4-byte
+// store per entry, and k_inval_unmark resets all caches with one sequential
+// fill. Only enabled where a recomputed gain equals the cached one for every
+// vertex whose neighbourhood did not change (a fixed filter ratio per level,
+// or the mapping objective).
 __device__ __forceinline__ bool scattered_inval(const JArgs &a) {
     return (unsigned long long) a.st->sum[SUM_PERF_ENTRIES] < a.inval_all_min;
 }
@@ -1006,7 +1035,7 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
     const bool inval = scattered_inval(a);
     const bool hub_upd = hub_update_now(a);
-    if (a.hub_stale && !hub_upd && blockIdx.x == 0 && threadIdx.x == 0) *a.hub_stale = 1u;
+    if (a.hub_cur && !hub_upd && blockIdx.x == 0 && threadIdx.x == 0) *a.hub_cur += 1u;
     const u64 stride = (u64) gridDim.x * blockDim.x;
     long long acc = 0;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < total; base += stride) {
@@ -1284,7 +1313,7 @@ __global__ void __launch_bounds__(BLOCK) k_rb_dispatch(JArgs a, RbArgs r) {
         if (cls == 1) a.heavy[s1] = u;
         u32 s2 = warp_append(&a.st->cnt[ST_HEAVY2], cls == 2);
         if (cls == 2) a.heavy2[s2] = u;
-        if (a.hubacc && !a.hub_stale) emit_hub_chunks(a, s2, cls == 2 ? a.g.rowlen[u] : 0u);
+        hub_dispatch(a, s2, cls == 2, u);
     }
 }
 
@@ -1385,7 +1414,6 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_tracked(JArgs a, u32 ratio, Rb
     const ConnTable<false, true> T{w, tv, 0, a.k};
     const u32 total = a.st->cnt[ST_HEAVY2];
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *a.hub_stale = 0u;  // the rebuild (if any) has finished
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         const u32 u = a.heavy2[i];
         const u32 hs = (u32) (a.dlab[u] >> DL_SLOT_SHIFT);
@@ -1401,8 +1429,8 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_tracked(JArgs a, u32 ratio, Rb
 }
 
 // Level set-up of tracked hubs: numbers the hub rows (rows of more than
-// hub_deg entries) and writes dlab for every vertex; emits the chunk items of
-// the hub rows for k_hub_build.
+// hub_deg entries), writes dlab for every vertex and sums the hub rows'
+// lengths into the status word's sum[0].
 __global__ void __launch_bounds__(BLOCK) k_hub_number(JArgs a) {
     const u64 stride = (u64) gridDim.x * blockDim.x;
     for (u64 base = (u64) blockIdx.x * blockDim.x; base < a.g.n; base += stride) {
@@ -1414,23 +1442,22 @@ __global__ void __launch_bounds__(BLOCK) k_hub_number(JArgs a) {
         if (ok) a.heavy2[slot] = u;
         if (ok) const_cast<u32 *>(a.hub_vertex)[slot] = u;
         if (u < a.g.n) a.dlab[u] = a.map[u] | (ok ? (unsigned long long) (slot + 1) << DL_SLOT_SHIFT : 0ull);
-        emit_hub_chunks(a, slot, ok ? a.g.rowlen[u] : 0u);
+        if (ok) atomicAdd((unsigned long long *) &a.st->sum[0], (unsigned long long) a.g.rowlen[u]);
     }
 }
 
-// Builds the tracked connectivity of every hub row from the chunk items of
-// all hub rows (a.hub_items); each warp adds its chunk's block sums to the
-// row's hubacc entries. With `only_if_stale`, does nothing unless the sums
-// were marked stale.
-__global__ void __launch_bounds__(JW_BLOCK) k_hub_build(JArgs a, int only_if_stale) {
-    if (only_if_stale && *(volatile u32 *) a.hub_stale == 0u) return;
+// Rebuilds the tracked connectivity of the hubs the dispatch found stale
+// (their sums zeroed there) from their chunk items; each warp adds its
+// chunk's block sums to the row's hubacc entries.
+__global__ void __launch_bounds__(JW_BLOCK) k_hub_rebuild(JArgs a) {
     u32 *w = warp_table<true>(a.k);
     s32 *tv = (s32 *) w;
-    const u32 total = a.hub_nitems;
+    u32 total = a.st->cnt[ST_CHUNKS];
+    if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
     const u32 lane = lane_id();
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
-        const unsigned long long it = a.hub_items[i];
+        const unsigned long long it = a.items[i];
         const u32 h = (u32) (it >> 32);
         const u32 u = a.hub_vertex[h];
         const u32 len = __ldg(&a.g.rowlen[u]);
@@ -1451,15 +1478,6 @@ __global__ void __launch_bounds__(JW_BLOCK) k_hub_build(JArgs a, int only_if_sta
 // dlab of every vertex without tracked hubs: the label alone.
 __global__ void k_dlab_init(JArgs a) {
     for (u32 u = blockIdx.x * blockDim.x + threadIdx.x; u < a.g.n; u += gridDim.x * blockDim.x) a.dlab[u] = a.map[u];
-}
-
-// Zeroes the tracked hub sums when they were marked stale (first half of a
-// rebuild; k_hub_build(a, 1) follows).
-__global__ void k_hub_zero(JArgs a) {
-    if (*(volatile u32 *) a.hub_stale == 0u) return;
-    const u64 total = (u64) a.hub_cap * a.k;
-    for (u64 i = (u64) blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (u64) gridDim.x * blockDim.x)
-        a.hubacc[i] = 0;
 }
 
 // underloaded_blocks (:614-627): ordered list of blocks below max_b_w.
@@ -2300,7 +2318,7 @@ JArgs make_args(JetLevel &L) {
     a.items = L.items;
     a.items_cap = L.items_cap;
     a.abacc = L.abacc;
-    a.inval_all_min = L.cache_pure ? (L.g.m + 1) / 2 : ~0ull;
+    a.inval_all_min = L.cache_pure ? (L.g.m * L.ctx->tune.jet_inval_all_pct + 99) / 100 : ~0ull;
     a.hubacc = L.hubacc;
     a.hubcnt = L.hubcnt;
     a.hub_cap = L.hub_cap;
@@ -2308,9 +2326,8 @@ JArgs make_args(JetLevel &L) {
     a.dlab = L.dlab;
     a.abrec = L.abrec;
     a.hub_track_max = L.hub_track_max;
-    a.hub_stale = L.hub_stale;
-    a.hub_items = L.hub_items;
-    a.hub_nitems = L.hub_nitems;
+    a.hub_cur = L.hub_cur;
+    a.hub_gen = L.hub_gen;
     a.hub_vertex = L.hub_vertex;
     a.abcnt = L.abcnt;
     a.st = L.ctx->d_status;
@@ -2468,9 +2485,8 @@ void JetLevel::setup(Ctx &c, const DGraph &gr, u32 kk, s32 lm, const DistOracle 
     hub_cap = 0;
     dlab = nullptr;
     abrec = nullptr;
-    hub_stale = nullptr;
-    hub_items = nullptr;
-    hub_nitems = 0;
+    hub_cur = nullptr;
+    hub_gen = nullptr;
     hub_vertex = nullptr;
     hub_track_max = 0;
     if (warp_direct && k <= HUB_K) {
@@ -2505,42 +2521,35 @@ void JetLevel::prepare_kernel_loop() {
         HP_LAUNCH_CHECK();
         return;
     }
-    hub_stale = c.balloc<u32>(1);
+    hub_cur = c.balloc<u32>(1);
+    hub_gen = c.balloc<u32>(hub_cap);
     u32 *vertex = c.balloc<u32>(hub_cap);
     hub_vertex = vertex;
-    HP_CUDA(cudaMemsetAsync(hub_stale, 0, sizeof(u32), c.stream));
+    // every hub starts stale: generation 0x01010101 against 0; the passes
+    // build the sums of the hubs they need
+    HP_CUDA(cudaMemsetAsync(hub_gen, 0, sizeof(u32) * hub_cap, c.stream));
+    HP_CUDA(cudaMemsetAsync(hub_cur, 1, sizeof(u32), c.stream));
     c.zero_counters();
     JArgs a = make_args(*this);
     k_hub_number<<<c.grid(g.n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
     HP_LAUNCH_CHECK();
-    // keep the hub rows' chunk items (the items array is reused by every pass)
     const DevStatus &st = c.read_status();
     if (st.err) throw HpError{HP_ERR_DEVICE, "hub numbering reported error bits " + std::to_string(st.err)};
-    hub_nitems = std::min<u32>(st.cnt[ST_CHUNKS], items_cap);
-    unsigned long long *its = c.balloc<unsigned long long>(hub_nitems);
-    HP_CUDA(cudaMemcpyAsync(its, items, sizeof(unsigned long long) * hub_nitems, cudaMemcpyDeviceToDevice, c.stream));
-    hub_items = its;
-    // sums of all hub rows' lengths: updates pay while the moved rows hold at
-    // most jet_hub_track_pct percent of that many entries
-    const unsigned long long hub_entries = (unsigned long long) hub_nitems * hub_deg;
+    // updates pay while the moved rows hold at most jet_hub_track_pct percent
+    // of the hub rows' entries
+    const unsigned long long hub_entries = (unsigned long long) st.sum[0];
     hub_track_max = hub_entries / 100 * c.tune.jet_hub_track_pct;
-    a = make_args(*this);
-    k_hub_build<<<c.grid((u64) hub_nitems * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(
-        a, 0);
-    note_launch();
-    HP_LAUNCH_CHECK();
     c.zero_counters();
 }
 
-// Rebuilds the tracked hub sums if the last perform marked them stale
-// (device-side check; no host synchronisation).
-void JetLevel::refresh_hubs() {
-    if (!hub_stale) return;
+// Rebuilds the sums of the stale hubs the pass's dispatch found (no host
+// synchronisation: the item count stays on the device).
+void JetLevel::rebuild_hubs() {
+    if (!hub_cur) return;
     Ctx &c = *ctx;
     JArgs a = make_args(*this);
-    k_hub_zero<<<c.grid((u64) hub_cap * k, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
-    k_hub_build<<<c.grid((u64) hub_nitems * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(
-        a, 1);
+    KernTimer kt(c, "k_hub_rebuild");
+    k_hub_rebuild<<<c.grid((u64) items_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32), c.stream>>>(a);
     note_launch();
 }
 
@@ -2550,11 +2559,11 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     JArgs a = make_args(*this);
     const u32 n = g.n;
     gain_rec = c.instr.begin(c.stream, "jet_gain", 0.0);
-    refresh_hubs();
     {
         KernTimer kt(c, "k_lp_dispatch");
         k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
     }
+    rebuild_hubs();
     {
         KernTimer kt(c, "k_lp_warp");
         if (warp_direct) {
@@ -2566,7 +2575,7 @@ void JetLevel::gain_pass(u32 ratio_pct) {
     }
     {
         KernTimer kt(c, "k_lp_block");
-        if (hub_stale) {
+        if (hub_cur) {
             k_hub_tracked<0><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                c.stream>>>(a, ratio_pct, RbArgs{});
         } else if (hubacc) {
@@ -2620,7 +2629,6 @@ void JetLevel::weak() {
     k_under<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, under, &c.d_status->cnt[ST_AUX]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, under, keys};
-    refresh_hubs();
     {
         ProfScope p2(c, "weak.pick");
         KernTimer kt(c, "k_weak_pick");
@@ -2628,6 +2636,7 @@ void JetLevel::weak() {
             KernTimer kt1(c, "k_weak_dispatch");
             k_rb_dispatch<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
         }
+        rebuild_hubs();
         {
             KernTimer kt1(c, "k_weak_warp");
             if (warp_direct) {
@@ -2639,7 +2648,7 @@ void JetLevel::weak() {
         }
         {
             KernTimer kt1(c, "k_weak_block");
-            if (hub_stale) {
+            if (hub_cur) {
                 k_hub_tracked<1><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                    c.stream>>>(a, 0u, r);
             } else if (hubacc) {
@@ -2709,7 +2718,6 @@ void JetLevel::strong() {
     k_maxv<<<1, 1024, 0, c.stream>>>(bw, k, max_b_w, &c.d_status->imax[1]); note_launch();
     JArgs a = make_args(*this);
     RbArgs r{opt, max_b_w, sections, nullptr, keys};
-    refresh_hubs();
     {
         ProfScope p2(c, "strong.pick");
         KernTimer kt(c, "k_strong_pick");
@@ -2717,6 +2725,7 @@ void JetLevel::strong() {
             KernTimer kt1(c, "k_strong_dispatch");
             k_rb_dispatch<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, r); note_launch();
         }
+        rebuild_hubs();
         {
             KernTimer kt1(c, "k_strong_warp");
             if (warp_direct) {
@@ -2728,7 +2737,7 @@ void JetLevel::strong() {
         }
         {
             KernTimer kt1(c, "k_strong_block");
-            if (hub_stale) {
+            if (hub_cur) {
                 k_hub_tracked<2><<<c.grid((u64) hub_cap * 32, JW_BLOCK), JW_BLOCK, (JW_BLOCK / 32) * k * sizeof(u32),
                                    c.stream>>>(a, 0u, r);
             } else if (hubacc) {
@@ -3079,7 +3088,8 @@ void jet_refine(Ctx &ctx, const DGraph &g, u32 *part, u32 k, s32 lmax, bool ultr
                 // entry of a moved row adj (+ ew), the neighbour's label and
                 // its cache reset
                 const double ent = (double) st.sum[SUM_PERF_ENTRIES];
-                const bool all = L.cache_pure && (u64) st.sum[SUM_PERF_ENTRIES] >= (g.m + 1) / 2;
+                const bool all = L.cache_pure &&
+                                 (u64) st.sum[SUM_PERF_ENTRIES] >= (g.m * ctx.tune.jet_inval_all_pct + 99) / 100;
                 ctx.instr.pending[L.delta_rec].bytes =
                     36.0 * nm + (g.ew ? 16.0 : 12.0) * ent - (all ? 4.0 * ent - 4.0 * g.n : 0.0);
             }

@@ -69,9 +69,8 @@ struct JetLevel {
     u32 hub_cap = 0;        // hub-row slots
     unsigned long long *dlab = nullptr;   // per-kernel loop: packed label / moved / old label / hub slot
     unsigned long long *abrec = nullptr;  // per-kernel loop: packed gain / target / label (afterburner)
-    u32 *hub_stale = nullptr;                         // tracked hubs: sums to be rebuilt before the next pass
-    const unsigned long long *hub_items = nullptr;    // tracked hubs: chunk items of all hub rows
-    u32 hub_nitems = 0;
+    u32 *hub_cur = nullptr;                           // tracked hubs: current generation of the sums (device word)
+    u32 *hub_gen = nullptr;                           // tracked hubs: generation each hub's sums were built for
     const u32 *hub_vertex = nullptr;                  // tracked hubs: row of each hub slot
     unsigned long long hub_track_max = 0;             // tracked hubs: update while moved entries <= this
     u32 hub_deg = 0;        // hub threshold and chunk length (entries)
@@ -99,12 +98,14 @@ struct JetLevel {
     // Single pass helpers used by tests: recompute gains for all vertices
     // whose cache is invalid (the "Jet-gain" kernel).
     // Before the per-kernel level loop: packed per-vertex words for the delta
-    // pass and the afterburner, and, with direct tables and k <= 256, the
-    // connectivity of every hub row (Tunables::jet_hub_conn), after which the
-    // delta pass keeps it up to date and the gain and rebalance passes read
-    // it instead of rescanning hub rows.
+    // pass and the afterburner, and, with direct tables and k <= 256, tracked
+    // connectivity of the hub rows (Tunables::jet_hub_conn): the gain and
+    // rebalance passes read a hub's k sums instead of rescanning its row, the
+    // delta pass keeps the sums up to date (or, after many moves, advances
+    // their generation), and a pass rebuilds the stale sums of the hubs it
+    // needs (rebuild_hubs, after its dispatch).
     void prepare_kernel_loop();
-    void refresh_hubs();
+    void rebuild_hubs();
     void gain_pass(u32 ratio_pct);
 
     // One Jet iteration: the step (0 = lp with ratio_pct, 1 = weak, 2 =

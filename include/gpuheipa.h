@@ -228,7 +228,11 @@ int hp_coop_slot_release(int device);
  * from the moved vertices instead of rescanning the rows every pass; 0: rescan),
  * "jet_hub_track_pct" (with jet_hub_conn = 1: a perform whose moved rows hold
  * more entries than this percentage of all hub-row entries lets the next pass
- * rebuild the hub sums from the rows instead of updating them).
+ * rebuild the hub sums from the rows instead of updating them),
+ * "jet_inval_all_pct" (1..100: where a recomputed gain equals a still-valid
+ * cached one, a perform whose moved rows hold at least this percentage of the
+ * level's entries resets every cached gain with one sequential fill instead of
+ * one scattered reset per entry of the moved rows).
  * Unknown names return HP_ERR_ARG. No counterpart in the reference. */
 int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
 

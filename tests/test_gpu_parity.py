@@ -368,6 +368,37 @@ def test_chunk_modes_equal_oracle(mode):
         c.close()
 
 
+@pytest.mark.parametrize("pct", [1, 100])
+def test_cache_reset_threshold_equal_oracle(pct):
+    # A perform resets every cached gain at once when its moved rows hold at
+    # least pct % of the level's entries (1: nearly every perform; 100: only
+    # when every row moved), else the neighbours of the moved rows one by
+    # one; cut (default and ultra, whose changing filter ratio keeps the
+    # scattered resets) and J.
+    cases = [(H.Graph.rmat(15, 16, 0.57, 0.19, 0.19, 1, 10, 3), 64, "default"),
+             (H.Graph.rmat(14, 16, seed=3), 32, "ultra"), (H.Graph.grid(120, 100, 1, 10, seed=4), 16, "default")]
+    m = H.Graph.rgg3d(20000, 14.0, 1, 100, seed=8, explicit_vw=True)
+    c = H.Context(0, 2 << 30)
+    try:
+        for name in ("jet_fused_max_n", "jet_coop_max_n"):
+            c.tune(name, 0)
+        c.tune("jet_inval_all_pct", pct)
+        for g, k, config in cases:
+            part, cut = c.partition(g, k, 0.03, config, 7)
+            opart, ocut = O.partition(to_oracle(g), k, 0.03, config == "ultra", 7)
+            assert cut == ocut
+            np.testing.assert_array_equal(part, opart)
+        mp, J = c.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, "HM", 3)
+        want_m, want_j = O.map_hm(to_oracle(m), [2, 4, 3], [1, 10, 100], 0.03, False, 3)
+        assert J == want_j
+        np.testing.assert_array_equal(mp, want_m)
+        for bad in (0, 101):
+            with pytest.raises(H.HeiPaError):
+                c.tune("jet_inval_all_pct", bad)
+    finally:
+        c.close()
+
+
 @pytest.mark.parametrize("hub_conn", [0, 1])
 def test_hub_rows_tracked_or_rescanned_equal_oracle(hub_conn):
     # The per-kernel Jet path with every row above 64 entries a hub: the hub
