@@ -674,6 +674,7 @@ int hp_tune(hp_ctx *ctx, const char *name, int64_t value) {
     else if (nm == "jet_hub_conn" && value <= 1) t.jet_hub_conn = (uint32_t) value;
     else if (nm == "jet_hub_track_pct") t.jet_hub_track_pct = (uint32_t) std::min<int64_t>(value, 1000000);
     else if (nm == "jet_inval_all_pct" && value >= 1 && value <= 100) t.jet_inval_all_pct = (uint32_t) value;
+    else if (nm == "jet_vec_loads" && value <= 1) t.jet_vec_loads = (uint32_t) value;
     else {
         ctx->c.last_error = "unknown tunable " + nm;
         return HP_ERR_ARG;

@@ -31,7 +31,12 @@ void Arena::init(size_t bytes) {
 }
 
 void Arena::attach(void *p, size_t bytes) {
-    base_ = (char *) p;
+    // every allocation is ALIGN-aligned (kernels read CSR arrays with 16-byte
+    // vector loads), so the base is rounded up to ALIGN
+    const uintptr_t at = ((uintptr_t) p + ALIGN - 1) & ~(uintptr_t) (ALIGN - 1);
+    const size_t skip = (size_t) (at - (uintptr_t) p);
+    bytes = bytes > skip ? bytes - skip : 0;
+    base_ = (char *) at;
     size_ = bytes & ~(ALIGN - 1);
     front_ = 0;
     back_ = size_;

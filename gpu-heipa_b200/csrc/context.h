@@ -140,6 +140,7 @@ struct Tunables {
     u32 jet_chunk_mode = 0;            // chunk kernels: 0 = 4 entries per lane, 1 = 8, 2 = bulk-copy staged rows
     u32 jet_hub_conn = 1;              // per-kernel Jet loop: keep hub-row connectivity up to date (1) or rescan (0)
     u32 jet_hub_track_pct = 50;        // ... updated while the moved rows hold <= this % of the hub-row entries
+    u32 jet_vec_loads = 1;             // Jet row passes read row entries as 16-byte quads (1) or 4-byte strided loads (0)
     u32 jet_inval_all_pct = 5;         // a perform whose moved rows hold >= this % of all entries resets every cache at once
 };
 

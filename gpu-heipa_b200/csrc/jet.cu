@@ -87,6 +87,9 @@ struct JArgs {
     // dest_part (next 16) and label (top 16) of a vertex, written by the
     // filter, so that a neighbour costs one gather. Null: separate arrays.
     unsigned long long *abrec;
+    // Row entries read as 16-byte quads (Tunables::jet_vec_loads) in the
+    // kernels that support it; else four strided 4-byte loads.
+    u32 vec;
     // Tracked hub connectivity (k <= HUB_K, hub_cur set): hubacc then
     // holds, for every hub row h and block b, the row's connection to b at
     // hubacc[h * k + b] (the two counters one moved neighbour changes share a
@@ -174,6 +177,48 @@ __device__ __forceinline__ void load_entries(const JArgs &a, u64 beg, u32 t0, u3
     }
 }
 
+// 128-bit row reads: the four CSR entries of quad qi (positions [4 qi,
+// 4 qi + 4)) with one 16-byte load of adj and one of ew; entries outside
+// [lo, hi) come back as SENTINEL with weight 0. Whole quads are read: CSR
+// arrays come from the arena, whose allocations are 256-byte aligned and
+// padded to 256 bytes, so a quad holding an entry lies inside its array's
+// allocation.
+__device__ __forceinline__ void load_quad(const JArgs &a, u64 qi, u64 lo, u64 hi, u32 (&v)[4], s32 (&w)[4]) {
+    const uint4 q = __ldg(reinterpret_cast<const uint4 *>(a.g.adj) + qi);
+    int4 r = make_int4(1, 1, 1, 1);
+    if (a.g.ew) r = __ldg(reinterpret_cast<const int4 *>(a.g.ew) + qi);
+    v[0] = q.x;
+    v[1] = q.y;
+    v[2] = q.z;
+    v[3] = q.w;
+    w[0] = r.x;
+    w[1] = r.y;
+    w[2] = r.z;
+    w[3] = r.w;
+    const u64 p = qi * 4;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (p + j < lo || p + j >= hi) {
+            v[j] = SENTINEL;
+            w[j] = 0;
+        }
+}
+
+// Quad qi of the entries [lo, hi) if it holds any of them (returns true),
+// else SENTINEL / 0 in v and w (returns false).
+__device__ __forceinline__ bool next_quad(const JArgs &a, u64 qi, u64 lo, u64 hi, u32 (&v)[4], s32 (&w)[4]) {
+    if (qi * 4 >= hi) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            v[j] = SENTINEL;
+            w[j] = 0;
+        }
+        return false;
+    }
+    load_quad(a, qi, lo, hi, v, w);
+    return true;
+}
+
 __device__ __forceinline__ u32 thash(u32 key, u32 mask) { return (key * 2654435761u >> 7) & mask; }
 
 __device__ __forceinline__ u32 table_mask_for(u32 len, u32 k, u32 cap) {
@@ -241,6 +286,36 @@ template<bool BLK, bool NC = true>
 __device__ __forceinline__ void dtable_build_range(const JArgs &a, u32 u, s32 *tv, u32 from, u32 len) {
     const u64 beg = __ldg(&a.g.rowptr[u]);
     const u32 gs = Grp<BLK>::size(), tid = Grp<BLK>::tid();
+    if (NC && a.vec) {
+        // the same with the entries read as 16-byte quads
+        const u64 lo = beg + from, hi = beg + len;
+        u64 qi = (lo >> 2) + tid;
+        u32 b[4];
+        s32 w[4];
+        if (next_quad(a, qi, lo, hi, b, w)) {
+            for (;;) {
+                const u64 qn = qi + gs;
+                u32 bn[4];
+                s32 wn[4];
+                const bool more = next_quad(a, qn, lo, hi, bn, wn);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (b[j] != EMPTY) b[j] = ldj<NC>(&a.map[b[j]]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if (b[j] != EMPTY) atomicAdd(&tv[b[j]], w[j]);
+                if (!more) break;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    b[j] = bn[j];
+                    w[j] = wn[j];
+                }
+                qi = qn;
+            }
+        }
+        Grp<BLK>::sync();
+        return;
+    }
     if (NC) {
         // kernels that do not write labels: the next four entries are loaded
         // while the current four labels are gathered
@@ -783,6 +858,35 @@ __device__ __forceinline__ s32 ab_range(const JArgs &a, u32 u, s32 ug, u32 ou, u
     return change;
 }
 
+// The same with 128-bit row reads (quads tid, tid + gs, ... of the segment).
+template<bool NC = true>
+__device__ __forceinline__ s32 ab_range_quads(const JArgs &a, u32 u, s32 ug, u32 ou, u32 nu, u32 from, u32 to,
+                                              u32 tid, u32 gs) {
+    const u64 beg = __ldg(&a.g.rowptr[u]);
+    const u64 lo = beg + from, hi = beg + to;
+    u64 qi = (lo >> 2) + tid;
+    u32 v[4];
+    s32 w[4];
+    if (!next_quad(a, qi, lo, hi, v, w)) return 0;
+    s32 change = 0;
+    for (;;) {
+        const u64 qn = qi + gs;
+        u32 vn[4];
+        s32 wn[4];
+        const bool more = next_quad(a, qn, lo, hi, vn, wn);
+        change = wadd(change, ab_batch<NC>(a, u, ug, ou, nu, v, w));
+        if (!more) break;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            v[j] = vn[j];
+            w[j] = wn[j];
+        }
+        qi = qn;
+    }
+    return change;
+}
+
+template<bool VEC>
 __global__ void __launch_bounds__(BLOCK) k_ab_thread(JArgs a) {
     __shared__ u32 sm[33];
     const u32 total = a.st->cnt[ST_CAND];
@@ -797,7 +901,9 @@ __global__ void __launch_bounds__(BLOCK) k_ab_thread(JArgs a) {
             if (len <= CHUNK_THREAD_MAX) {
                 const s32 ug = __ldg(&a.gain1[u]);
                 const u32 ou = __ldg(&a.map[u]), nu = __ldg(&a.dest_part[u]);
-                if (wadd(ug, ab_range(a, u, ug, ou, nu, 0, len, 0, 1)) >= 0) {
+                const s32 ch = VEC ? ab_range_quads(a, u, ug, ou, nu, 0, len, 0, 1)
+                                   : ab_range(a, u, ug, ou, nu, 0, len, 0, 1);
+                if (wadd(ug, ch) >= 0) {
                     a.lock[u] = 1;
                     lock = true;
                 }
@@ -815,6 +921,7 @@ __global__ void __launch_bounds__(BLOCK) k_ab_thread(JArgs a) {
 // row of several chunks each warp adds its partial sum to abacc[u] and the
 // last warp to finish (counted in abcnt[u], after a fence) decides and resets
 // both words, so nothing waits for another warp.
+template<bool VEC>
 __global__ void __launch_bounds__(BLOCK, 4) k_ab_chunk(JArgs a) {
     u32 total = a.st->cnt[ST_HEAVY];
     if (total > a.items_cap) total = a.items_cap;
@@ -824,7 +931,9 @@ __global__ void __launch_bounds__(BLOCK, 4) k_ab_chunk(JArgs a) {
         chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
         const s32 ug = __ldg(&a.gain1[u]);
         const u32 ou = __ldg(&a.map[u]), nu = __ldg(&a.dest_part[u]);
-        const s32 change = (s32) warp_sum<u32>((u32) ab_range<true, true>(a, u, ug, ou, nu, from, to, lane_id(), 32));
+        const s32 part = VEC ? ab_range_quads(a, u, ug, ou, nu, from, to, lane_id(), 32)
+                             : ab_range<true, true>(a, u, ug, ou, nu, from, to, lane_id(), 32);
+        const s32 change = (s32) warp_sum<u32>((u32) part);
         if (lane_id() == 0) {
             bool decide = nch == 1;
             s32 tot = change;
@@ -959,6 +1068,40 @@ __device__ __forceinline__ long long delta_range(const JArgs &a, u32 u, u32 from
     return acc;
 }
 
+// The same with 128-bit row reads: thread tid of a group of gs takes quads
+// tid, tid + gs, ... of the row segment, the next quad loaded while the
+// current one's labels are gathered.
+template<bool NC = true>
+__device__ __forceinline__ long long delta_range_quads(const JArgs &a, u32 u, u32 from, u32 to, u32 tid, u32 gs,
+                                                       bool inval, bool hub_upd) {
+    const u64 beg = __ldg(&a.g.rowptr[u]);
+    const u32 x = ldj<NC>(&a.map[u]);
+    const bool um = (x & MOVED) != 0;
+    const u32 nu = x & ~MOVED;
+    const u32 ou = um ? ldj<NC>(&a.dest_part[u]) : nu;
+    const u64 lo = beg + from, hi = beg + to;
+    u64 qi = (lo >> 2) + tid;
+    u32 v[4];
+    s32 w[4];
+    if (!next_quad(a, qi, lo, hi, v, w)) return 0;
+    long long acc = 0;
+    for (;;) {
+        const u64 qn = qi + gs;
+        u32 vn[4];
+        s32 wn[4];
+        const bool more = next_quad(a, qn, lo, hi, vn, wn);
+        acc += delta_batch<4, NC>(a, nu, ou, um, v, w, inval, hub_upd);
+        if (!more) break;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            v[j] = vn[j];
+            w[j] = wn[j];
+        }
+        qi = qn;
+    }
+    return acc;
+}
+
 // The same over len entries staged in shared memory (one warp, B per lane).
 template<int B>
 __device__ __forceinline__ long long delta_staged(const JArgs &a, u32 u, const u32 *sadj, const s32 *sew, u32 len,
@@ -1031,6 +1174,7 @@ __device__ __forceinline__ void block_add_s64(long long v, long long *dst) {
     }
 }
 
+template<bool VEC>
 __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
     const u32 total = a.st->cnt[ST_MOVES];
     const bool inval = scattered_inval(a);
@@ -1044,7 +1188,9 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
         if (i < total) {
             u = a.moves[i];
             const u32 len = __ldg(&a.g.rowlen[u]);
-            if (len <= CHUNK_THREAD_MAX) acc += delta_range(a, u, 0, len, 0, 1, inval, hub_upd);
+            if (len <= CHUNK_THREAD_MAX)
+                acc += VEC ? delta_range_quads(a, u, 0, len, 0, 1, inval, hub_upd)
+                           : delta_range(a, u, 0, len, 0, 1, inval, hub_upd);
             else nch = chunks_of(len);
         }
         warp_emit_chunks(a, u, nch, &a.st->cnt[ST_HEAVY]);
@@ -1070,8 +1216,8 @@ __global__ void __launch_bounds__(BLOCK) k_delta_thread(JArgs a) {
 // gathers, so resident warps matter more than registers. The objective delta
 // is added with one atomic per warp, so no warp waits for the others of its
 // block at the end.
-template<int B>
-__global__ void __launch_bounds__(BLOCK, B > 4 ? 4 : 5) k_delta_chunk(JArgs a) {
+template<int B, bool VEC = false>
+__global__ void __launch_bounds__(BLOCK, (B > 4 || VEC) ? 4 : 5) k_delta_chunk(JArgs a) {
     u32 total = a.st->cnt[ST_HEAVY];
     if (total > a.items_cap) total = a.items_cap;
     const u32 warps = (gridDim.x * blockDim.x) >> 5;
@@ -1081,7 +1227,8 @@ __global__ void __launch_bounds__(BLOCK, B > 4 ? 4 : 5) k_delta_chunk(JArgs a) {
     for (u32 i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < total; i += warps) {
         u32 u, from, to, nch;
         chunk_range(a, __ldg(&a.items[i]), u, from, to, nch);
-        acc += delta_range<true, B, B <= 4>(a, u, from, to, lane_id(), 32, inval, hub_upd);
+        if (VEC) acc += delta_range_quads(a, u, from, to, lane_id(), 32, inval, hub_upd);
+        else acc += delta_range<true, B, B <= 4>(a, u, from, to, lane_id(), 32, inval, hub_upd);
     }
     acc = warp_sum<long long>(acc);
     if (lane_id() == 0 && acc) atomicAdd((unsigned long long *) &a.st->sum[SUM_DELTA], (unsigned long long) acc);
@@ -2325,6 +2472,7 @@ JArgs make_args(JetLevel &L) {
     a.hub_deg = L.hub_deg;
     a.dlab = L.dlab;
     a.abrec = L.abrec;
+    a.vec = L.ctx->tune.jet_vec_loads;
     a.hub_track_max = L.hub_track_max;
     a.hub_cur = L.hub_cur;
     a.hub_gen = L.hub_gen;
@@ -2604,11 +2752,15 @@ void JetLevel::lp(u32 ratio_pct) {
     KernTimer kt(c, "k_afterburner");
     {
         KernTimer kt1(c, "k_ab_thread");
-        k_ab_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        if (a.vec) k_ab_thread<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+        else k_ab_thread<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+        note_launch();
     }
     {
         KernTimer kt1(c, "k_ab_chunk");
-        k_ab_chunk<<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+        if (a.vec) k_ab_chunk<true><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+        else k_ab_chunk<false><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+        note_launch();
     }
     HP_LAUNCH_CHECK();
 }
@@ -2833,7 +2985,9 @@ void JetLevel::perform() {
         delta_rec = kt.idx;
         {
             KernTimer kt1(c, "k_delta_thread");
-            k_delta_thread<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a); note_launch();
+            if (a.vec) k_delta_thread<true><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+            else k_delta_thread<false><<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a);
+            note_launch();
         }
         {
             KernTimer kt1(c, "k_delta_chunk");
@@ -2844,7 +2998,8 @@ void JetLevel::perform() {
             } else if (c.tune.jet_chunk_mode == 1) {
                 k_delta_chunk<8><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
             } else {
-                k_delta_chunk<4><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+                if (a.vec) k_delta_chunk<4, true><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
+                else k_delta_chunk<4><<<c.grid((u64) items_cap * 32, BLOCK), BLOCK, 0, c.stream>>>(a);
             }
             note_launch();
         }

@@ -232,7 +232,10 @@ int hp_coop_slot_release(int device);
  * "jet_inval_all_pct" (1..100: where a recomputed gain equals a still-valid
  * cached one, a perform whose moved rows hold at least this percentage of the
  * level's entries resets every cached gain with one sequential fill instead of
- * one scattered reset per entry of the moved rows).
+ * one scattered reset per entry of the moved rows), "jet_vec_loads" (1: the
+ * Jet row passes read CSR entries as 16-byte quads of four, one vector load
+ * of adj and one of ew per lane; 0: four strided 4-byte loads; values above
+ * 1 are rejected).
  * Unknown names return HP_ERR_ARG. No counterpart in the reference. */
 int hp_tune(hp_ctx *ctx, const char *name, int64_t value);
 
