@@ -2711,7 +2711,11 @@ void JetLevel::gain_pass(u32 ratio_pct) {
         KernTimer kt(c, "k_lp_dispatch");
         k_lp_dispatch<<<c.grid(n, BLOCK), BLOCK, 0, c.stream>>>(a, ratio_pct); note_launch();
     }
+    // the hub sums the pass needs are rebuilt under their own timer (the
+    // gain pass's algorithmic bytes count a tracked hub as its k sums)
+    c.instr.end(c.stream, gain_rec);
     rebuild_hubs();
+    const size_t gain_rec2 = c.instr.begin(c.stream, "jet_gain", 0.0);
     {
         KernTimer kt(c, "k_lp_warp");
         if (warp_direct) {
@@ -2735,7 +2739,7 @@ void JetLevel::gain_pass(u32 ratio_pct) {
         note_launch();
     }
     HP_LAUNCH_CHECK();
-    c.instr.end(c.stream, gain_rec);
+    c.instr.end(c.stream, gain_rec2);
 }
 
 void JetLevel::lp(u32 ratio_pct) {
