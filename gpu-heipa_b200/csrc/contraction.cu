@@ -4,6 +4,9 @@
 // table (<= 256), a per-block shared-memory table (<= 4096) or a global hash
 // table (larger), and written straight into the padded coarse CSR at the
 // capacity offsets.
+#include <algorithm>
+#include <vector>
+
 #include "coarsen.cuh"
 #include "prims.cuh"
 
@@ -23,6 +26,7 @@ constexpr u32 C_BLOCK_SMALL_BITS = 11;
 constexpr int C_WARP_BLOCK = 128;  // 4 warps per block for the warp kernel
 constexpr int C_HUGE_BLOCK = 1024;
 constexpr int C_ST_BLOCK_LARGE = 3;  // status slot: clusters of the large block tier
+constexpr int C_ST_HUGE_TICKET = 4;  // status slot: next huge cluster to be taken by a block
 
 __device__ __forceinline__ u32 hslot(u32 key, u32 bits) { return (key * 2654435761u) >> (32 - bits); }
 
@@ -59,6 +63,7 @@ struct TierLists {
     u32 *bl, *bcnt;    // block tier, 2048-slot tables
     u32 *bl2, *b2cnt;  // block tier, 8192-slot tables
     u32 *hl, *hcnt;    // huge clusters
+    u32 *hcap;         // huge clusters: row capacity (entries of the member rows)
     u32 *hoffc;        // per coarse vertex: offset of its global table (huge clusters)
     unsigned long long *hbump;  // global table slots handed out
 };
@@ -140,7 +145,10 @@ __global__ void k_contract_small(CArgs a, TierLists L) {
         u32 s4 = warp_append(L.b2cnt, cls == 4);
         if (cls == 4) L.bl2[s4] = c;
         u32 s3 = warp_append(L.hcnt, cls == 3);
-        if (cls == 3) L.hl[s3] = c;
+        if (cls == 3) {
+            L.hl[s3] = c;
+            L.hcap[s3] = cap;
+        }
     }
     msum = warp_sum<unsigned long long>(msum);
     if (lane_id() == 0 && msum) atomicAdd(a.m_out, msum);
@@ -334,12 +342,19 @@ struct HugeSlot {
     s32 w;
 };
 
+// Blocks take clusters from hl (largest first) through a ticket, so that no
+// block is left with several large clusters while others are idle.
 __global__ void __launch_bounds__(C_HUGE_BLOCK) k_contract_huge(CArgs a, const u32 *hl, const u32 *hcnt,
-                                                               const u32 *hoff, HugeSlot *slots) {
+                                                               const u32 *hoff, HugeSlot *slots, u32 *ticket) {
     __shared__ u32 scan_sm[32];
+    __shared__ u32 s_next;
     const u32 total = *hcnt;
     unsigned long long msum = 0;
-    for (u32 i = blockIdx.x; i < total; i += gridDim.x) {
+    for (;;) {
+        if (threadIdx.x == 0) s_next = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const u32 i = s_next;
+        if (i >= total) break;
         const u32 c = hl[i];
         const u32 cap = a.c.rowptr[c + 1] - a.c.rowptr[c];
         const u32 tsz = 2 * cap;
@@ -417,6 +432,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     u32 *bl = ctx.balloc<u32>(n_c);
     u32 *bl2 = ctx.balloc<u32>(n_c);
     u32 *hl = ctx.balloc<u32>(n_c);
+    u32 *hcap = ctx.balloc<u32>(n_c);
     u32 *hoffc = ctx.balloc<u32>(n_c);
     HP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(u32) * n_c, ctx.stream));
     HP_CUDA(cudaMemsetAsync(capsum, 0, sizeof(u32) * n_c, ctx.stream));
@@ -442,7 +458,7 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
     CArgs a{g, mapping, moff, mlist, c, &st->err, (unsigned long long *) &st->sum[1]};
     const size_t rec0 = ctx.instr.begin(ctx.stream, "contract", 0.0);
     const size_t rec_t = ctx.instr.begin(ctx.stream, "contract_thread", 0.0);
-    TierLists TL{wl, &st->cnt[0], bl, &st->cnt[1], bl2, &st->cnt[C_ST_BLOCK_LARGE], hl, &st->cnt[2], hoffc,
+    TierLists TL{wl, &st->cnt[0], bl, &st->cnt[1], bl2, &st->cnt[C_ST_BLOCK_LARGE], hl, &st->cnt[2], hcap, hoffc,
                  (unsigned long long *) &st->sum[0]};
     k_contract_small<<<ctx.grid(n_c, BLOCK), BLOCK, 0, ctx.stream>>>(a, TL); note_launch();
     HP_LAUNCH_CHECK();
@@ -477,11 +493,22 @@ DGraph contract_graph(Ctx &ctx, const DGraph &g, const u32 *mapping, u32 n_c) {
         HP_LAUNCH_CHECK();
     }
     if (nh) {
+        // largest clusters first (their rows differ by two orders of
+        // magnitude; a block that took a large one late would finish alone)
+        std::vector<u32> hv(nh), hc(nh), order(nh);
+        HP_CUDA(cudaMemcpyAsync(hv.data(), hl, sizeof(u32) * nh, cudaMemcpyDeviceToHost, ctx.stream));
+        HP_CUDA(cudaMemcpyAsync(hc.data(), hcap, sizeof(u32) * nh, cudaMemcpyDeviceToHost, ctx.stream));
+        ctx.sync();
+        for (u32 i = 0; i < nh; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](u32 x, u32 y) { return hc[x] != hc[y] ? hc[x] > hc[y] : hv[x] < hv[y]; });
+        for (u32 i = 0; i < nh; ++i) hc[i] = hv[order[i]];
+        HP_CUDA(cudaMemcpyAsync(hl, hc.data(), sizeof(u32) * nh, cudaMemcpyHostToDevice, ctx.stream));
+        ctx.sync();
         HugeSlot *slots = ctx.balloc<HugeSlot>(hslots);
         KernTimer kt(ctx, "contract");
         KernTimer kt1(ctx, "contract_huge");
         k_contract_huge<<<(u32) std::min<u64>(nh, (u64) ctx.sm_count * 2), C_HUGE_BLOCK, 0, ctx.stream>>>(
-            a, hl, &st->cnt[2], hoffc, slots); note_launch();
+            a, hl, &st->cnt[2], hoffc, slots, &st->cnt[C_ST_HUGE_TICKET]); note_launch();
         HP_LAUNCH_CHECK();
     }
     const DevStatus &s2 = ctx.read_status();

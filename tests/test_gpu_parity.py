@@ -368,6 +368,33 @@ def test_chunk_modes_equal_oracle(mode):
         c.close()
 
 
+def test_scalar_row_reads_equal_oracle():
+    # The Jet row passes with four strided 4-byte loads per lane instead of
+    # 16-byte quads (jet_vec_loads = 0): weighted and unit-weight R-MAT with
+    # hub rows, a grid, and J.
+    cases = [(H.Graph.rmat(15, 16, 0.57, 0.19, 0.19, 1, 10, 3), 64, "default"),
+             (H.Graph.rmat(14, 16, seed=3), 32, "ultra"), (H.Graph.grid(120, 100, 1, 10, seed=4), 16, "default")]
+    m = H.Graph.rgg3d(20000, 14.0, 1, 100, seed=8, explicit_vw=True)
+    c = H.Context(0, 2 << 30)
+    try:
+        for name in ("jet_fused_max_n", "jet_coop_max_n"):
+            c.tune(name, 0)
+        c.tune("jet_vec_loads", 0)
+        for g, k, config in cases:
+            part, cut = c.partition(g, k, 0.03, config, 7)
+            opart, ocut = O.partition(to_oracle(g), k, 0.03, config == "ultra", 7)
+            assert cut == ocut
+            np.testing.assert_array_equal(part, opart)
+        mp, J = c.process_map(m, [2, 4, 3], [1, 10, 100], 0.03, "IM", 3)
+        want_m, want_j = O.map_im(to_oracle(m), [2, 4, 3], [1, 10, 100], 0.03, 3)
+        assert J == want_j
+        np.testing.assert_array_equal(mp, want_m)
+        with pytest.raises(H.HeiPaError):
+            c.tune("jet_vec_loads", 2)
+    finally:
+        c.close()
+
+
 @pytest.mark.parametrize("pct", [1, 100])
 def test_cache_reset_threshold_equal_oracle(pct):
     # A perform resets every cached gain at once when its moved rows hold at
