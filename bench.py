@@ -571,9 +571,9 @@ def run_ours(args, world, rank, local):
 
 
 def run_quality(args, world, rank, local):
-    """Quality over seeds 1..N (north star check (d)): the objective of every
-    seed on the GPU and, with --quality-oracle, of the CPU oracle restatement
-    on the same graph and seed, with the geometric means."""
+    """Quality over seeds 1..N: the objective of every seed on the GPU and,
+    with --quality-oracle, of the CPU oracle restatement on the same graph
+    and seed, with the geometric means."""
     if rank != 0:
         return 0
     import gpu_heipa as H
