@@ -2,13 +2,15 @@
 // (src/refinement/jet_label_propagation.h) and for the process-mapping
 // objective J(C,D,Pi) (src/refinement/promap_jet_label_propagation.h).
 //
-// Connectivity rows are not stored: every pass that needs conn(u, b) for a
-// vertex aggregates it on the fly from the CSR row and the current labels
-// (registers for degree <= 16, a per-warp shared-memory hash table for
-// degree <= 512, a per-block table beyond). The dest/gain cache of the
-// reference (dest_cache/gain_cache, invalidated when the vertex or one of its
-// neighbours moves) is kept, so a pass only reaches vertices whose
-// neighbourhood changed.
+// Connectivity rows are not stored for ordinary vertices: every pass that
+// needs conn(u, b) aggregates it on the fly from the CSR row and the current
+// labels (registers for degree <= 16, a per-warp shared-memory table up to
+// the hub threshold, hub rows in chunks). Hub rows of the per-kernel level
+// loop (k <= 256) keep their k block sums instead, updated by the delta pass
+// or rebuilt per hub when stale (JetLevel::prepare_kernel_loop). The
+// dest/gain cache of the reference (dest_cache/gain_cache, invalidated when
+// the vertex or one of its neighbours moves) is kept, so a pass only reaches
+// vertices whose neighbourhood changed.
 #pragma once
 #include "graph.cuh"
 
