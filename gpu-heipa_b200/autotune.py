@@ -1,8 +1,11 @@
 """Autotuner for the launch-structure thresholds of the partitioner
 (hp_tune): which levels replay their Jet iterations as CUDA graphs, which
-rebalance steps order candidates in one block, and which matching loops run
-as one cooperative launch. Every setting gives identical results (they only
-change how the same kernels are launched), so tuning is a pure timing search.
+rebalance steps order candidates in one block, which matching loops run as
+one cooperative launch, and how the Jet row passes work (hub-row tracking,
+when a perform resets every cached gain at once, 16-byte or 4-byte row
+reads, entries per lane). Every setting gives identical results (they only
+change how the same results are computed), so tuning is a pure timing
+search.
 
     import gpu_heipa as H, autotune
     ctx = H.Context(0, 8 << 30)
@@ -28,11 +31,17 @@ CANDIDATES = {
     "jet_coop_max_deg": [16, 32, 64],
     "jet_coop_rows": [512, 1024, 2048],
     "jet_hub_deg": [256, 1024, 4096],
+    "jet_hub_conn": [0, 1],
+    "jet_hub_track_pct": [25, 50, 100],
+    "jet_inval_all_pct": [1, 5, 50],
+    "jet_vec_loads": [0, 1],
+    "jet_chunk_mode": [0, 1],
 }
 DEFAULTS = {"jet_graph_max_m": 1 << 24, "order_small_n": 16384, "match_coop_max_n": 1 << 17,
             "match_coop_max_m": 1 << 21, "jet_fused_max_n": 4096, "jet_fused_max_m": 1 << 18,
             "jet_coop_max_n": 65536, "jet_coop_max_m": 1 << 21, "jet_coop_max_deg": 32, "jet_coop_rows": 1024,
-            "jet_hub_deg": 1024}
+            "jet_hub_deg": 1024, "jet_hub_conn": 1, "jet_hub_track_pct": 50, "jet_inval_all_pct": 5,
+            "jet_vec_loads": 1, "jet_chunk_mode": 0}
 
 
 def _time(ctx, graphs, ks, config, seed, repeats):
